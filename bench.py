@@ -1,0 +1,379 @@
+#!/usr/bin/env python
+"""Headline benchmark: GTEPS of the out-of-HBM frontier engine on one B200.
+
+Default workload (N=1): directed RMAT scale 24, edge factor 16 (a=.57,
+b=.19, c=.19), self-loops/duplicates removed, ids permuted, WCSR with
+weights in [1,64]; the HBM edge budget holds 40% of the edge bytes, the rest
+is read zero-copy from pinned host memory.  A step is one SSSP from source 1
+(bit-exact distances).  The second algorithm of the same configuration, CC
+(min-label propagation) on the symmetrised graph with the same 40% budget,
+is reported under "extra".
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                  [--workload c2|c1|c3]
+
+value: whole-job GTEPS = traversed edges (sum of out-degrees of the vertices
+the source reaches, each counted once) / device time, summed over ranks
+(weak scaling: every rank runs its own replica; the path does not shard).
+e2e: the same metric through the C ABI with a host output buffer, host
+wall-clock, device->host copy of the values inside the timed region.
+--impl reference: the CPU oracle (OpenMP, all host threads) on the same
+workload -- the reference has no CPU implementation of this path.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SEED = 0x54484592
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--scale", type=int, default=0, help="override the workload's scale")
+    ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+WORKLOADS = {
+    # name: (algo, scale, edge_factor, fmt, symmetric, budget_frac, budget_bytes)
+    "c1": dict(algo="bfs", scale=20, ef=16, fmt="csr", sym=False, frac=1.0),
+    "c2": dict(algo="sssp", scale=24, ef=16, fmt="wcsr", sym=False, frac=0.4),
+    "c2cc": dict(algo="cc", scale=24, ef=16, fmt="csr", sym=True, frac=0.4),
+    "c3": dict(algo="pr_pull", scale=26, ef=16, fmt="csc", sym=False, budget=2 << 30),
+}
+
+
+class Dist:
+    def __init__(self, n):
+        self.n = n
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.pg = None
+        if self.world > 1:
+            import torch.distributed as dist
+            import datetime
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x):
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), f[5], f[6], f[7], f[8], float(f[3])))
+            except ValueError:
+                pass
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = []
+        for i, name in [(2, "hw_slowdown"), (3, "hw_thermal_slowdown"), (4, "sw_thermal_slowdown"),
+                        (5, "sw_power_cap")]:
+            if any(r[i].lower().startswith("active") for r in rows):
+                reasons.append(name)
+        busy = [r[0] for r in rows if r[6] > 250] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic_bytes(off, vals, nv, vb, res, esz, algo, n_iters=1):
+    """Per-run bytes a work-optimal run must move, split HBM / host link.
+
+    BFS/SSSP: every reached vertex is expanded once: 16 B of offsets and a
+    4 B value write, its adjacency (esz per edge; over the host link when its
+    block is not resident) and a 4 B value probe per edge.  CC/PR: every
+    vertex once per iteration (CC: the synchronous label-propagation sweep
+    count is not fixed, so the bytes of ONE full sweep are used -- a lower
+    bound)."""
+    deg = np.diff(off.astype(np.int64))
+    if algo in ("bfs", "sssp"):
+        mask = vals < nv + 1
+    else:
+        mask = np.ones(nv, bool)
+    blk = np.searchsorted(vb.astype(np.int64), np.arange(nv), side="right") - 1
+    resident_v = res[blk]
+    d = deg[mask]
+    r = resident_v[mask]
+    per_edge_probe = 4 if algo != "pr_push" else 8
+    link = int((d[~r] * esz).sum())
+    hbm = int((d[r] * esz).sum() + d.sum() * per_edge_probe + mask.sum() * (16 + 4))
+    return hbm * n_iters, link * n_iters, int(d.sum())
+
+
+def run_ours(args, dist):
+    import torch
+    import thievory_b200 as T
+    from oracle import oracle as O
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    T.load_library()
+    hbm_peak, peak_kind = peaks()
+    wl = dict(WORKLOADS[args.workload])
+    if args.scale:
+        wl["scale"] = args.scale
+    result = {}
+
+    link_mc, link_zc = T.link_bandwidth(dev, 1 << 30)
+    link_peak = max(link_mc, link_zc)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    stream = torch.cuda.Stream(device=dev)
+
+    def measure(wl, k, w, want_e2e, want_cpu):
+        g = T.Graph.generate_rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"],
+                                  fmt=wl["fmt"], device=dev)
+        budget = wl.get("budget", int(wl.get("frac", 1.0) * g.ne * g.esz))
+        plan = g.plan(budget)
+        algo = wl["algo"]
+        src = 1
+        sptr = stream.cuda_stream
+        for _ in range(w):
+            g.run(algo, source=src, want_values=False, stream=sptr)
+        vals = g.values(algo)
+        off, edges, _ = g.host_arrays()
+        vb, res = g.blocks()
+        iters = 20 if algo.startswith("pr") else 1
+        b_hbm, b_link, trav = algorithmic_bytes(off, vals if algo in ("bfs", "sssp") else None,
+                                                g.nv, vb, res, g.esz, algo, iters)
+        if algo == "cc" or algo.startswith("pr"):
+            trav = g.ne * iters
+        clocks = Clocks(dev)
+        clocks.start()
+        dist.barrier()
+        torch.cuda.synchronize(dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        lib_ms, launches, link_bytes, hbm_bytes = [], 0, 0, 0
+        with torch.cuda.stream(stream):
+            for i in range(k):
+                flush.zero_()  # > L2 write between steps (outside the events)
+                ev[i][0].record(stream)
+                _, st = g.run(algo, source=src, want_values=False, stream=sptr)
+                ev[i][1].record(stream)
+                lib_ms.append(st["device_ms"])
+                launches += st["kernel_launches"]
+                link_bytes += st["link_edge_bytes"]
+                hbm_bytes += st["hbm_edge_bytes"]
+        stream.synchronize()
+        dist.barrier()
+        ck = clocks.stop()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        total_s = dist.max(sum(step_ms) / 1e3)
+        value = dist.n * trav * k / total_s / 1e9
+        t_roof = b_hbm / (hbm_peak * 1e9) + b_link / (link_peak * 1e9)
+        kern_s = statistics.mean(lib_ms) / 1e3
+        out = {
+            "value": value, "ms_per_step": total_s * 1e3 / k, "traversed_edges": trav,
+            "plan": plan, "clocks": ck, "gpu_launches": launches,
+            "roofline": {
+                "bound": "hbm", "unit": "GB/s",
+                "achieved": (b_hbm + b_link) / kern_s / 1e9,
+                "peak": (b_hbm + b_link) / t_roof / 1e9,
+                "frac": t_roof / kern_s,
+                "traffic": None,
+                "algorithmic_hbm_bytes": b_hbm, "algorithmic_link_bytes": b_link,
+                "hbm_peak_gbs": hbm_peak, "hbm_peak_kind": peak_kind,
+                "link_peak_gbs": link_peak, "link_memcpy_gbs": link_mc, "link_zerocopy_gbs": link_zc,
+                "kernel_ms": kern_s * 1e3,
+                "actual_link_bytes_per_step": link_bytes // k,
+                "actual_hbm_edge_bytes_per_step": hbm_bytes // k,
+                "note": "mixed bound: peak = bytes / (B_hbm/HBM + B_link/link); frac = T_roof / T",
+            },
+        }
+        if want_e2e:
+            host = torch.empty(g.nv * (2 if algo.startswith("pr") else 1), dtype=torch.int32).pin_memory()
+            hv = host.numpy().view(np.float64 if algo.startswith("pr") else np.uint32)
+            wall = []
+            for _ in range(k):
+                t0 = time.perf_counter()
+                _, st = g.run(algo, source=src, out=hv, stream=sptr)
+                wall.append(time.perf_counter() - t0)
+            tw = dist.max(sum(wall))
+            out["e2e"] = {"value": dist.n * trav * k / tw / 1e9, "unit": "GTEPS",
+                          "h2d_bytes_per_step": int(st["link_edge_bytes"] + st["h2d_bytes"]),
+                          "d2h_bytes_per_step": int(st["d2h_bytes"]),
+                          "note": "h2d = zero-copy edge bytes read over the host link"}
+            if algo in ("bfs", "sssp", "cc"):
+                assert np.array_equal(hv, vals), "e2e values differ from device run"
+        if want_cpu and dist.rank == 0 and dist.n == 1:
+            L = O.lib()
+            cv = np.empty(g.nv, np.uint32)
+            P = lambda a: None if a is None else a.ctypes.data
+            t0 = time.perf_counter()
+            if algo == "sssp":
+                L.thvo_sssp_par(g.nv, P(off), P(edges), None, 2, src, P(cv))
+            elif algo == "bfs":
+                L.thvo_bfs_par(g.nv, P(off), P(edges), 1, src, P(cv))
+            elif algo == "cc":
+                L.thvo_cc_par(g.nv, P(off), P(edges), 1, P(cv))
+            dt = time.perf_counter() - t0
+            if algo in ("bfs", "sssp", "cc"):
+                assert np.array_equal(cv, vals), "GPU result differs from the CPU oracle"
+            out["cpu_baseline"] = {"value": trav / dt / 1e9, "unit": "GTEPS", "cores": O.threads(),
+                                   "kind": "port",
+                                   "sample": f"one full {algo} run of this workload on the host "
+                                             f"(OpenMP oracle, {dt:.2f} s); result checked equal"}
+        g.close()
+        return out
+
+    main = measure(wl, args.steps, args.warmup, True, not args.no_cpu)
+    extra = {}
+    if args.workload == "c2" and not args.no_extra:
+        cc = measure(dict(WORKLOADS["c2cc"], scale=wl["scale"]), args.steps, args.warmup, False,
+                     not args.no_cpu)
+        extra["cc_rmat_sym_40pct"] = {k: cc[k] for k in ("value", "ms_per_step", "traversed_edges",
+                                                          "roofline", "gpu_launches")}
+        if "cpu_baseline" in cc:
+            extra["cc_rmat_sym_40pct"]["cpu_baseline"] = cc["cpu_baseline"]
+    return wl, main, extra
+
+
+def run_reference(args, dist):
+    """CPU oracle (the reference has no CPU path) on the same workload."""
+    from oracle import oracle as O
+
+    wl = dict(WORKLOADS[args.workload])
+    if args.scale:
+        wl["scale"] = args.scale
+    g = O.rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"], weighted=wl["algo"] == "sssp")
+    algo = wl["algo"]
+    fn = {"sssp": lambda: O.sssp(g, 1, parallel=True), "bfs": lambda: O.bfs(g, 1, parallel=True),
+          "cc": lambda: O.cc(g, parallel=True),
+          "pr_pull": lambda: O.pagerank(g, 20)}[algo]
+    for _ in range(args.warmup):
+        vals = fn()
+    t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        vals = fn()
+        t.append(time.perf_counter() - t0)
+    trav = O.reached_edges(g, vals) if algo in ("bfs", "sssp") else g.ne * (20 if algo.startswith("pr") else 1)
+    value = trav / statistics.mean(t) / 1e9
+    return wl, value, statistics.mean(t) * 1e3, O.threads()
+
+
+def main():
+    args = parse()
+    dist = Dist(args.gpus)
+    if args.impl == "reference":
+        if dist.rank != 0:
+            dist.close()
+            return
+        wl, value, ms, cores = run_reference(args, dist)
+        line = {"metric": f"GTEPS ({wl['algo']})", "value": value, "unit": "GTEPS", "impl": "reference",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                "data": "synthetic (seeded RMAT, CPU generator)",
+                "config": {"workload": f"{wl['algo']} rmat{wl['scale']} ef{wl['ef']}"},
+                "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "port",
+                                 "sample": f"full {wl['algo']} run per step on the host (OpenMP oracle)"},
+                "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        dist.close()
+        return
+    wl, m, extra = run_ours(args, dist)
+    if dist.rank == 0:
+        budget_desc = (f"{int(wl['frac'] * 100)}% of edge bytes" if "frac" in wl else f"{wl['budget']} bytes")
+        line = {
+            "metric": f"GTEPS ({wl['algo']})", "value": m["value"], "unit": "GTEPS",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded RMAT a=.57 b=.19 c=.19, dedup, no self-loops, permuted ids)",
+            "config": {"workload": f"{wl['algo']} rmat{wl['scale']} ef{wl['ef']} {wl['fmt']} "
+                                   f"hbm-budget {budget_desc}",
+                       "scale": wl["scale"], "edge_factor": wl["ef"], "format": wl["fmt"],
+                       "hbm_edge_budget": budget_desc, "source": 1,
+                       "resident_edge_bytes": m["plan"]["resident_edge_bytes"],
+                       "host_edge_bytes": m["plan"]["host_edge_bytes"],
+                       "traversed_edges_per_step": m["traversed_edges"],
+                       "parallelism": f"replicas x{args.gpus}",
+                       "l2": "256 MiB device write between timed steps (outside the events)"},
+            "roofline": m["roofline"], "gpu_launches": m["gpu_launches"],
+            "clocks": m["clocks"], "e2e": m.get("e2e"),
+        }
+        if "cpu_baseline" in m:
+            line["cpu_baseline"] = m["cpu_baseline"]
+        if extra:
+            line["extra"] = extra
+        print(json.dumps(line))
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

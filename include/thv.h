@@ -1,0 +1,240 @@
+/*
+ * thv.h -- C ABI of the B200 out-of-memory graph engine (thievory_b200).
+ *
+ * Plain C, no CUDA or torch types: the CLI (`./main`), the Python host mirror
+ * (thievory_b200/__init__.py, via ctypes), tests and bench.py all call these.
+ *
+ * Conventions
+ *   - Every call returns thv_status; the library never calls exit() and never
+ *     lets a C++ exception cross this boundary.  thv_last_error() gives a
+ *     thread-local message for the last failing call on that thread.
+ *   - The caller owns output buffers; the library owns device memory and the
+ *     pinned host copy of the edges.
+ *   - A thv_graph is used by one host thread at a time.  The serving API
+ *     (thv_serve_*) is internally multi-threaded and may be called from any
+ *     thread.
+ *
+ * Reference interfaces replaced (paths inside qqueke/Thievory):
+ *   thv_open / thv_close        CSR<E>::ReadInputFile  src/graph.cuh:641-815,
+ *                               CSR<E>::Free           src/graph.cuh:855-923
+ *   thv_plan                    CSR<E>::InitData / SetPartitionsConfig /
+ *                               SetNumStaticEdges      src/graph.cuh:270-638
+ *   thv_run                     BFS32 src/bfs/bfs.cu:8, CC32 src/cc/cc.cu:71,
+ *                               SSSP32 src/sssp/sssp.cu:10, PR32 src/pr/pr.cu:11,
+ *                               PR32_PUSH src/pr/pr.cu:1030
+ *   thv_values / thv_write_values
+ *                               CSR<E>::DumpValues     src/graph.cuh:817-852
+ *   thv_save                    converter/converter.cpp:483-589 (.csc),
+ *                               :676-774 (.csr), :775-805 (.wcsr)
+ *   thv_batch_run, thv_serve_*, thv_generate_rmat
+ *                               no counterpart in the reference (new surface)
+ */
+#ifndef THV_H
+#define THV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define THV_ABI_VERSION 1
+
+typedef enum thv_status {
+  THV_OK = 0,
+  THV_EINVAL = 1,       /* bad argument (null pointer, source >= n, ...) */
+  THV_EIO = 2,          /* file cannot be opened, read or written */
+  THV_EFORMAT = 3,      /* truncated or malformed graph file */
+  THV_ENOMEM = 4,       /* device / pinned allocation failed, or over budget */
+  THV_ECUDA = 5,        /* CUDA runtime error (message in thv_last_error) */
+  THV_ETIMEOUT = 6,     /* a bounded device wait or iteration cap ran out */
+  THV_EUNSUPPORTED = 7, /* option combination not supported */
+  THV_EBUSY = 8,        /* serving: queue full / not admitted */
+  THV_ENOTREADY = 9,    /* serving: result not ready yet */
+  THV_EDEVICE = 10      /* kernel reported an internal error (queue overflow) */
+} thv_status;
+
+/* File / in-memory layouts (converter byte formats). */
+typedef enum thv_format {
+  THV_FMT_CSR = 0,  /* u64 nv, u64 ne, u64 off[nv], u32 dst[ne], u32 w[ne] */
+  THV_FMT_CSC = 1,  /* u64 nv, u64 ne, u64 in_off[nv], u32 src[ne], u32 outdeg[nv] */
+  THV_FMT_WCSR = 2  /* u64 nv, u64 ne, u64 off[nv], {u32 dst, u32 w}[ne] */
+} thv_format;
+
+/* thv_open flags */
+#define THV_OPEN_WEIGHTS 1u /* CSR: load the trailing weight section (SSSP) */
+
+typedef enum thv_algo {
+  THV_ALGO_BFS = 0,     /* u32 levels: source 1, unreached n+1 */
+  THV_ALGO_CC = 1,      /* u32 labels: min id of any vertex reaching v */
+  THV_ALGO_SSSP = 2,    /* u32: min(distance + 1, n+1); needs weights */
+  THV_ALGO_PR_PUSH = 3, /* double ranks (FP32 on device); CSR input */
+  THV_ALGO_PR_PULL = 4  /* double ranks (FP32 on device); CSC input */
+} thv_algo;
+
+typedef struct thv_graph thv_graph;
+
+/* ---- graphs ---- */
+thv_status thv_open(const char *path, thv_format fmt, uint32_t flags,
+                    int device, thv_graph **out);
+
+/* Build from host arrays (copied).  off has nv+1 entries (off[nv] = ne).
+ * edges: u32 ids (esz 4) or interleaved {dst,w} pairs (esz 8, WCSR).
+ * outdeg: required for THV_FMT_CSC (in-edge graphs), else NULL. */
+thv_status thv_from_arrays(uint64_t nv, uint64_t ne, const uint64_t *off,
+                           const void *edges, uint32_t esz, thv_format fmt,
+                           const uint32_t *outdeg, int device,
+                           thv_graph **out);
+
+typedef struct thv_rmat_opts {
+  uint32_t scale;       /* nv = 2^scale */
+  uint32_t edge_factor; /* raw edges = edge_factor * nv (before dedup) */
+  uint64_t seed;
+  double a, b, c;       /* quadrant probabilities (d = 1 - a - b - c) */
+  uint32_t symmetric;   /* insert every edge both ways (CC) */
+  uint32_t pad;
+} thv_rmat_opts;
+
+/* Seeded RMAT on the GPU: self-loops and duplicates removed, ids permuted,
+ * CSR sorted by (src,dst); WCSR adds weights in [1,64]; CSC is the transpose
+ * with out-degrees.  Byte-identical to the CPU oracle's generator. */
+thv_status thv_generate_rmat(const thv_rmat_opts *o, thv_format fmt,
+                             int device, thv_graph **out);
+
+thv_status thv_save(const thv_graph *g, const char *path);
+thv_status thv_close(thv_graph *g);
+
+typedef struct thv_graph_info {
+  uint64_t nv, ne;
+  uint32_t fmt, esz;    /* in-memory edge size: 4 or 8 */
+  uint32_t device, weighted;
+} thv_graph_info;
+thv_status thv_info(const thv_graph *g, thv_graph_info *out);
+/* Host views of the graph (valid until thv_close). outdeg NULL unless CSC. */
+thv_status thv_host_arrays(const thv_graph *g, const uint64_t **off,
+                           const void **edges, const uint32_t **outdeg);
+
+/* ---- placement plan (static HBM budget) ---- */
+#define THV_PLACE_DENSEST 0u /* resident blocks chosen by edges per vertex */
+#define THV_PLACE_PREFIX 1u  /* longest prefix of blocks (reference order) */
+
+typedef struct thv_plan_opts {
+  uint64_t hbm_budget_bytes; /* resident edge bytes; UINT64_MAX = all that fit */
+  uint64_t block_bytes;      /* edge block size; 0 = 64 MiB */
+  uint32_t policy;
+  uint32_t pad;
+} thv_plan_opts;
+
+typedef struct thv_plan_info {
+  uint64_t num_blocks, resident_blocks;
+  uint64_t resident_edge_bytes, host_edge_bytes;
+  uint64_t device_bytes; /* all device memory the graph holds */
+} thv_plan_info;
+
+thv_status thv_plan(thv_graph *g, const thv_plan_opts *o); /* NULL = defaults */
+thv_status thv_get_plan(const thv_graph *g, thv_plan_info *out);
+/* Block table of the current plan: vbegin[0..nb] (first vertex of each
+ * block, vbegin[nb] = nv) and resident[0..nb-1] (1 = held in HBM).  cap is
+ * the capacity of resident (vbegin needs cap + 1); *nb receives the count. */
+thv_status thv_get_blocks(const thv_graph *g, uint64_t cap, uint32_t *vbegin,
+                          uint8_t *resident, uint64_t *nb);
+
+/* ---- single-source / whole-graph runs ---- */
+typedef struct thv_run_opts {
+  uint32_t source;       /* BFS / SSSP */
+  uint32_t pr_iters;     /* 0 = 20 */
+  double pr_damping;     /* 0 = 0.85 */
+  uint32_t sssp_delta;   /* near/far split width; 0 = auto */
+  uint32_t timeout_ms;   /* bound on any device-side wait; 0 = 60000 */
+  void *stream;          /* cudaStream_t to launch on; NULL = graph's own */
+  uint32_t small_degree; /* expansion tuning; 0 = default */
+  uint32_t chunk_edges;  /* expansion tuning; 0 = default */
+} thv_run_opts;
+
+typedef struct thv_stats {
+  double device_ms;         /* CUDA-event time of the traversal */
+  double wall_ms;           /* host time of the whole call */
+  uint64_t iterations;
+  uint64_t edges_expanded;  /* adjacency entries actually scanned */
+  uint64_t hbm_edge_bytes;  /* adjacency bytes read from resident blocks */
+  uint64_t link_edge_bytes; /* adjacency bytes read over the host link */
+  uint64_t h2d_bytes;       /* explicit host->device copies in the call */
+  uint64_t d2h_bytes;       /* explicit device->host copies in the call */
+  uint32_t kernel_launches;
+  uint32_t pad;
+} thv_stats;
+
+/* Runs algo.  out_values (host, may be NULL) receives u32[nv] or double[nv]
+ * (PR).  stats may be NULL.  Synchronous. */
+thv_status thv_run(thv_graph *g, thv_algo algo, const thv_run_opts *o,
+                   void *out_values, thv_stats *stats);
+/* Copy the last run's values (u32[nv], or double[nv] for PR) to the host. */
+thv_status thv_values(thv_graph *g, void *out_values);
+/* Write values as the reference does (headerless raw array). */
+thv_status thv_write_values(const char *path, const void *values, uint64_t n,
+                            uint32_t elem_size);
+
+/* ---- batched multi-source BFS / SSSP ---- */
+typedef struct thv_batch_opts {
+  uint32_t group;        /* sources per group, 1..64; 0 = 64 */
+  uint32_t timeout_ms;   /* 0 = 60000 */
+  void *stream;
+  uint32_t tuned;        /* 1 = use the autotuner's choice (default) */
+  uint32_t pad;
+} thv_batch_opts;
+
+/* out: n x nv u32 values, row i = result for sources[i], in the plain
+ * encoding (bit-exact equal to thv_run of that source). */
+thv_status thv_batch_run(thv_graph *g, thv_algo algo, const uint32_t *sources,
+                         uint32_t n, const thv_batch_opts *o, uint32_t *out,
+                         thv_stats *stats);
+
+/* ---- serving (continuous batching) ---- */
+typedef struct thv_server thv_server;
+
+typedef struct thv_serve_opts {
+  uint32_t max_slots;       /* concurrent queries on the device, <= 64 */
+  uint32_t queue_capacity;  /* pending requests; 0 = 4096 */
+  uint64_t mem_budget_bytes;/* device memory for per-query state; 0 = auto */
+  uint32_t timeout_ms;
+  uint32_t pad;
+} thv_serve_opts;
+
+typedef struct thv_query_stats {
+  double submit_to_start_ms, start_to_done_ms, latency_ms;
+  uint32_t iterations;
+  uint32_t slot;
+} thv_query_stats;
+
+thv_status thv_serve_start(thv_graph *g, const thv_serve_opts *o,
+                           thv_server **out);
+/* algo BFS or SSSP. Never blocks; THV_EBUSY when the queue is full. */
+thv_status thv_serve_submit(thv_server *s, thv_algo algo, uint32_t source,
+                            uint64_t *ticket);
+/* THV_ENOTREADY until done; then copies u32[nv] into out (may be NULL) and
+ * releases the ticket. */
+thv_status thv_serve_poll(thv_server *s, uint64_t ticket, uint32_t *out,
+                          thv_query_stats *st);
+thv_status thv_serve_wait(thv_server *s, uint64_t ticket, uint32_t *out,
+                          thv_query_stats *st, uint32_t timeout_ms);
+thv_status thv_serve_stop(thv_server *s);
+
+/* ---- misc ---- */
+/* Host-link bandwidth of `device` in GB/s: a pinned cudaMemcpy host->device
+ * of `bytes`, and a kernel streaming 16-byte zero-copy loads from pinned,
+ * mapped host memory (the engine's non-resident edge path).  Either output
+ * may be NULL. */
+thv_status thv_link_bandwidth(int device, uint64_t bytes, double *memcpy_gbs,
+                              double *zerocopy_gbs);
+const char *thv_last_error(void);
+const char *thv_status_str(thv_status s);
+uint32_t thv_abi_version(void);
+/* Host fault injection for tests: the n-th subsequent pinned/device
+ * allocation made by the library fails (0 disables). */
+void thv_debug_fail_alloc_after(uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* THV_H */

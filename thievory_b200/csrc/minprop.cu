@@ -1,0 +1,539 @@
+// Frontier engine for the monotone min-propagation family: BFS, CC, SSSP.
+//
+// Replaces the reference's per-level host loop (src/bfs/bfs.cu:55-524,
+// src/cc/cc.cu:71-614, src/sssp/sssp.cu:10-570) and its static / demand /
+// filter kernels (src/bfs/bfs_kernels.cu:4-287, src/cc/cc_kernels.cu:4-269,
+// src/sssp/sssp_kernels.cu:4-229) with ONE persistent cooperative kernel:
+//
+//   iteration i:
+//     compaction  - scan the pending-vertex bitmap 32 words per warp; ballot /
+//                   popc compaction of the taken vertices into two work
+//                   queues: "small" vertices (degree < small_degree), served
+//                   32 per warp with warp-cooperative load balancing, and
+//                   fixed-size edge chunks of high-degree vertices, one chunk
+//                   per warp with 128-byte aligned 16-byte vector loads.  A
+//                   word with no pending vertex costs one load: whole edge
+//                   blocks without an active source are never touched.
+//     grid barrier
+//     expansion   - warps pull tasks from an atomic counter; each edge does
+//                   "if (cand < val[w]) atomicMin; mark w pending".
+//     grid barrier
+//
+// The relaxation is the reference's (bfs_kernels.cu:63-70: new value < old
+// => atomicMin + frontier flag).  Its fixed point is unique, so results are
+// bit-exact whatever the schedule: BFS level+1, CC min reaching id, SSSP
+// min(dist+1, n+1).  SSSP takes only pending vertices below a moving
+// threshold (near/far split) to avoid re-expanding vertices whose distance
+// is still falling.
+//
+// Each vertex's adjacency is addressed through its edge block's base
+// address: resident blocks point into the HBM buffer, the others into the
+// pinned, mapped host copy, which the same load instructions read over the
+// host link (zero copy).
+#include <algorithm>
+#include <cstring>
+
+#include "thv_device.cuh"
+#include "thv_internal.h"
+
+namespace thv {
+
+enum { OP_BFS = 0, OP_CC = 1, OP_SSSP = 2 };
+
+constexpr int kMinThreads = 512;
+constexpr uint32_t kSmemBlocks = 2048;  // block table kept in shared memory
+constexpr uint32_t kDefaultSmall = 64;  // degree < this: warp-cooperative
+constexpr uint32_t kDefaultChunk = 256; // edges per high-degree work item
+
+struct __align__(16) WorkItem {
+  uint64_t eaddr;  // address of the first edge (device or host-mapped)
+  uint32_t v;
+  uint32_t cnt;
+};
+
+struct MinCtrl {
+  GridBar bar;
+  unsigned err, iters;
+  unsigned long long cnt_small[3], cnt_big[3], remaining[3], wc[3];
+  unsigned minkept[3], pad;
+  unsigned long long edges, hbm_bytes, link_bytes, vertices;
+};
+
+struct MinArgs {
+  uint32_t *val;
+  uint32_t *bm;
+  const uint64_t *off;
+  const uint32_t *blk_vb;
+  const uint64_t *blk_base;
+  uint64_t host_base;
+  WorkItem *qs, *qb;
+  unsigned long long cap_s, cap_b;
+  MinCtrl *ctrl;
+  unsigned long long timeout_ns;
+  uint32_t nblk, nv, ngroups, max_iters;
+  uint32_t delta, small_deg, chunk, src;
+};
+
+struct MinState {
+  uint64_t nv = 0;
+  uint32_t *d_val = nullptr;
+  uint32_t *d_bm = nullptr;
+  WorkItem *d_qs = nullptr, *d_qb = nullptr;
+  uint64_t cap_s = 0, cap_b = 0;
+  uint32_t chunk = 0, small = 0;
+  MinCtrl *d_ctrl = nullptr;
+  MinCtrl *h_ctrl = nullptr;  // pinned
+  uint32_t ngroups = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool valid = false;
+};
+
+__device__ __forceinline__ uint32_t find_block(const uint32_t *vb, uint32_t nblk,
+                                               uint32_t v) {
+  uint32_t lo = 0, hi = nblk;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (vb[mid] <= v) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ void relax(const MinArgs &a, uint32_t w,
+                                      unsigned long long cand) {
+  uint32_t *vp = a.val + w;
+  if (cand < ldcg(vp)) {
+    const uint32_t old = atomicMin(vp, (uint32_t)cand);
+    if (cand < old) {
+      const uint32_t m = 1u << (w & 31u);
+      uint32_t *bp = a.bm + (w >> 5);
+      if (!(ldcg(bp) & m)) atomicOr(bp, m);
+    }
+  }
+}
+
+template <int OP, int ESZ>
+__device__ __forceinline__ void relax_vec(const MinArgs &a, uint4 q,
+                                          uintptr_t p, uintptr_t start,
+                                          uintptr_t end, uint32_t vval) {
+  if (ESZ == 4) {
+    const uint32_t e[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const uintptr_t ea = p + 4u * j;
+      if (ea >= start && ea < end) {
+        const unsigned long long cand =
+            OP == OP_BFS ? (unsigned long long)vval + 1ull : vval;
+        relax(a, e[j], cand);
+      }
+    }
+  } else {
+    const uint32_t d[2] = {q.x, q.z}, wt[2] = {q.y, q.w};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      const uintptr_t ea = p + 8u * j;
+      if (ea >= start && ea < end) {
+        const unsigned long long cand =
+            OP == OP_BFS    ? (unsigned long long)vval + 1ull
+            : OP == OP_SSSP ? (unsigned long long)vval + wt[j]
+                            : (unsigned long long)vval;
+        relax(a, d[j], cand);
+      }
+    }
+  }
+}
+
+template <int OP, int ESZ>
+__device__ void process_chunk(const MinArgs &a, const WorkItem &it) {
+  const unsigned lane = lane_id();
+  const uint32_t vval = ldcg(a.val + it.v);
+  const uintptr_t start = it.eaddr;
+  const uintptr_t end = start + (uintptr_t)it.cnt * ESZ;
+  for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end;
+       p += 512u) {
+    const uint4 q = ld_nc_v4(p);
+    relax_vec<OP, ESZ>(a, q, p, start, end, vval);
+  }
+}
+
+template <int OP, int ESZ>
+__device__ void process_group(const MinArgs &a, unsigned long long first,
+                              unsigned long long n_small) {
+  const unsigned lane = lane_id();
+  const unsigned long long idx = first + lane;
+  WorkItem it{0, 0, 0};
+  uint32_t vval = 0;
+  if (idx < n_small) {
+    it = a.qs[idx];
+    vval = ldcg(a.val + it.v);
+  }
+  const unsigned incl = warp_incl_scan<unsigned>(it.cnt);
+  const unsigned excl = incl - it.cnt;
+  const unsigned total = __shfl_sync(kFull, incl, 31);
+  for (unsigned k = 0; k < total; k += 32) {
+    const unsigned t = k + lane;
+    const int o = warp_owner(excl, t);
+    const unsigned long long ea = shfl64(it.eaddr, o);
+    const unsigned oex = __shfl_sync(kFull, excl, o);
+    const uint32_t ov = __shfl_sync(kFull, vval, o);
+    if (t < total) {
+      const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
+      if (ESZ == 4) {
+        const uint32_t w = ld_nc_u32(addr);
+        const unsigned long long cand =
+            OP == OP_BFS ? (unsigned long long)ov + 1ull : ov;
+        relax(a, w, cand);
+      } else {
+        const uint2 e = ld_nc_u2(addr);
+        const unsigned long long cand =
+            OP == OP_BFS    ? (unsigned long long)ov + 1ull
+            : OP == OP_SSSP ? (unsigned long long)ov + e.y
+                            : (unsigned long long)ov;
+        relax(a, e.x, cand);
+      }
+    }
+  }
+}
+
+template <int OP, int ESZ>
+__global__ void __launch_bounds__(kMinThreads)
+    minprop_kernel(MinArgs a) {
+  extern __shared__ uint32_t s_vb[];
+  const bool smem_tab = a.nblk <= kSmemBlocks;
+  if (smem_tab)
+    for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x)
+      s_vb[i] = a.blk_vb[i];
+  __syncthreads();
+  const uint32_t *vb = smem_tab ? s_vb : a.blk_vb;
+  MinCtrl *c = a.ctrl;
+  const unsigned lane = lane_id();
+  const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+
+  uint32_t thr = 0xFFFFFFFFu;
+  if (OP == OP_SSSP) thr = (uint32_t)min(1ull + a.delta, 0xFFFFFFFFull);
+
+  unsigned iter = 0;
+  for (;; ++iter) {
+    if (iter >= a.max_iters) {
+      if (leader) atomicCAS(&c->err, 0u, kDevErrIters);
+      break;
+    }
+    const unsigned slot = iter % 3, nslot = (iter + 1) % 3;
+    if (leader) {
+      c->cnt_small[nslot] = 0;
+      c->cnt_big[nslot] = 0;
+      c->remaining[nslot] = 0;
+      c->wc[nslot] = 0;
+      c->minkept[nslot] = 0xFFFFFFFFu;
+    }
+    // ---------------------------------------------------------- compaction
+    unsigned long long my_edges = 0, my_hbm = 0, my_link = 0, my_verts = 0;
+    unsigned long long my_keep = 0;
+    uint32_t my_min = 0xFFFFFFFFu;
+    for (unsigned g = gwarp; g < a.ngroups; g += nwarps) {
+      const unsigned wbase = g * 32u;
+      const uint32_t word = ldcg(a.bm + wbase + lane);
+      unsigned nz = __ballot_sync(kFull, word != 0);
+      while (nz) {
+        const int j = __ffs(nz) - 1;
+        nz &= nz - 1;
+        const uint32_t wd = __shfl_sync(kFull, word, j);
+        const uint32_t v = (wbase + j) * 32u + lane;
+        const bool act = (wd >> lane) & 1u;
+        bool take = act;
+        uint32_t vval = 0;
+        if (OP == OP_SSSP && act) {
+          vval = ldcg(a.val + v);
+          take = vval < thr;
+        }
+        const unsigned tm = __ballot_sync(kFull, take);
+        if (OP == OP_SSSP) {
+          const bool kept = act && !take;
+          my_min = min(my_min, kept ? vval : 0xFFFFFFFFu);
+          if (lane == 0) my_keep += __popc(wd & ~tm);
+        }
+        if (lane == 0 && tm) a.bm[wbase + j] = wd & ~tm;
+        uint32_t deg = 0;
+        unsigned long long eaddr = 0;
+        if (take) {
+          const uint64_t s = __ldg(a.off + v), e = __ldg(a.off + v + 1);
+          deg = (uint32_t)(e - s);
+          const uint32_t b = find_block(vb, a.nblk, v);
+          const unsigned long long base = __ldg(a.blk_base + b);
+          eaddr = base + s * ESZ;
+          my_edges += deg;
+          my_verts += 1;
+          if (base == a.host_base) my_link += (unsigned long long)deg * ESZ;
+          else my_hbm += (unsigned long long)deg * ESZ;
+        }
+        const bool small = take && deg > 0 && deg < a.small_deg;
+        const bool big = take && deg >= a.small_deg;
+        const unsigned sm = __ballot_sync(kFull, small);
+        if (sm) {
+          const int ldr = __ffs(sm) - 1;
+          unsigned long long base = 0;
+          if (lane == (unsigned)ldr)
+            base = atomicAdd(&c->cnt_small[slot], (unsigned long long)__popc(sm));
+          base = shfl64(base, ldr);
+          const unsigned long long pos = base + __popc(sm & lanemask_lt());
+          if (small) {
+            if (pos < a.cap_s) a.qs[pos] = WorkItem{eaddr, v, deg};
+            else atomicCAS(&c->err, 0u, kDevErrQueue);
+          }
+        }
+        if (__any_sync(kFull, big)) {
+          const unsigned nch = big ? (deg + a.chunk - 1) / a.chunk : 0u;
+          const unsigned inc = warp_incl_scan<unsigned>(nch);
+          const unsigned tot = __shfl_sync(kFull, inc, 31);
+          unsigned long long base = 0;
+          if (lane == 0) base = atomicAdd(&c->cnt_big[slot], (unsigned long long)tot);
+          base = shfl64(base, 0);
+          if (big) {
+            unsigned long long pos = base + inc - nch;
+            for (unsigned k = 0; k < nch; k++, pos++) {
+              const uint32_t lo = k * a.chunk;
+              const uint32_t cnt = min(a.chunk, deg - lo);
+              if (pos < a.cap_b)
+                a.qb[pos] = WorkItem{eaddr + (unsigned long long)lo * ESZ, v, cnt};
+              else
+                atomicCAS(&c->err, 0u, kDevErrQueue);
+            }
+          }
+        }
+      }
+    }
+    my_edges = warp_sum(my_edges);
+    my_hbm = warp_sum(my_hbm);
+    my_link = warp_sum(my_link);
+    my_verts = warp_sum(my_verts);
+    if (OP == OP_SSSP) my_min = warp_min(my_min);
+    if (lane == 0 && my_verts) {
+      atomicAdd(&c->edges, my_edges);
+      atomicAdd(&c->hbm_bytes, my_hbm);
+      atomicAdd(&c->link_bytes, my_link);
+      atomicAdd(&c->vertices, my_verts);
+    }
+    if (OP == OP_SSSP && lane == 0) {
+      if (my_keep) atomicAdd(&c->remaining[slot], my_keep);
+      if (my_min != 0xFFFFFFFFu) atomicMin(&c->minkept[slot], my_min);
+    }
+    if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+
+    const unsigned long long ns = ldcg(&c->cnt_small[slot]);
+    const unsigned long long nb = ldcg(&c->cnt_big[slot]);
+    if (ns + nb == 0) {
+      if (OP != OP_SSSP) break;
+      if (ldcg(&c->remaining[slot]) == 0) break;
+      const uint32_t mk = ldcg(&c->minkept[slot]);
+      thr = (uint32_t)min((unsigned long long)mk + a.delta, 0xFFFFFFFFull);
+      continue;
+    }
+    // ----------------------------------------------------------- expansion
+    const unsigned long long ntask = nb + (ns + 31) / 32;
+    for (;;) {
+      unsigned long long t = 0;
+      if (lane == 0) t = atomicAdd(&c->wc[slot], 1ull);
+      t = shfl64(t, 0);
+      if (t >= ntask) break;
+      if (t < nb) {
+        const WorkItem it = a.qb[t];
+        process_chunk<OP, ESZ>(a, it);
+      } else {
+        process_group<OP, ESZ>(a, (t - nb) * 32ull, ns);
+      }
+    }
+    if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+  }
+  if (leader) c->iters = iter;
+}
+
+template <int OP>
+__global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t v = tid; v < a.nv; v += stride)
+    a.val[v] = OP == OP_CC ? (uint32_t)v : (v == a.src ? 1u : a.nv + 1u);
+  for (uint64_t w = tid; w < nw_alloc; w += stride) {
+    uint32_t word = 0;
+    if (OP == OP_CC) {
+      const uint64_t lo = w * 32ull;
+      if (lo + 32 <= a.nv) word = 0xFFFFFFFFu;
+      else if (lo < a.nv) word = (1u << (a.nv - lo)) - 1u;
+    } else if (w == (a.src >> 5)) {
+      word = 1u << (a.src & 31u);
+    }
+    a.bm[w] = word;
+  }
+  if (tid == 0) {
+    MinCtrl *c = a.ctrl;
+    memset(c, 0, sizeof(MinCtrl));
+    for (int s = 0; s < 3; s++) c->minkept[s] = 0xFFFFFFFFu;
+  }
+}
+
+// ------------------------------------------------------------------ host --
+
+static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
+                                   uint32_t small) {
+  MinState *&ms = g->ms;
+  if (ms && ms->valid && ms->chunk == chunk && ms->small == small) return THV_OK;
+  if (ms) minprop_free(g);
+  ms = new MinState();
+  ms->nv = g->nv;
+  ms->chunk = chunk;
+  ms->small = small;
+  const uint64_t nw = (g->nv + 31) / 32;
+  ms->ngroups = (uint32_t)((nw + 31) / 32);
+  const uint64_t nw_alloc = (uint64_t)ms->ngroups * 32;
+  ms->cap_s = g->nv + 32;
+  // every pending vertex of degree >= small yields ceil(deg/chunk) items
+  ms->cap_b = g->ne / chunk + g->ne / std::max<uint32_t>(small, 1) + 64;
+  THV_TRY(dev_alloc((void **)&ms->d_val, g->nv * 4 + 64, "values"));
+  THV_TRY(dev_alloc((void **)&ms->d_bm, nw_alloc * 4, "pending bitmap"));
+  THV_TRY(dev_alloc((void **)&ms->d_qs, ms->cap_s * sizeof(WorkItem), "queue"));
+  THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(WorkItem), "chunk queue"));
+  THV_TRY(dev_alloc((void **)&ms->d_ctrl, sizeof(MinCtrl), "control"));
+  THV_TRY(pinned_alloc((void **)&ms->h_ctrl, sizeof(MinCtrl), "control"));
+  THV_CUDA(cudaEventCreate(&ms->ev0));
+  THV_CUDA(cudaEventCreate(&ms->ev1));
+  ms->valid = true;
+  return THV_OK;
+}
+
+void minprop_free(thv_graph *g) {
+  MinState *ms = g->ms;
+  if (!ms) return;
+  dev_free(ms->d_val);
+  dev_free(ms->d_bm);
+  dev_free(ms->d_qs);
+  dev_free(ms->d_qb);
+  dev_free(ms->d_ctrl);
+  pinned_free(ms->h_ctrl);
+  if (ms->ev0) cudaEventDestroy(ms->ev0);
+  if (ms->ev1) cudaEventDestroy(ms->ev1);
+  delete ms;
+  g->ms = nullptr;
+}
+
+template <int OP, int ESZ>
+static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
+                                 uint32_t &launches) {
+  auto kern = minprop_kernel<OP, ESZ>;
+  const size_t smem =
+      g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0;
+  int bpsm = 0;
+  THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern,
+                                                         kMinThreads, smem));
+  if (bpsm < 1) return fail(THV_ECUDA, "minprop kernel cannot be resident");
+  const int grid = bpsm * g->num_sms;
+  const uint32_t nw_alloc = g->ms->ngroups * 32u;
+  const int init_grid = std::max(1, std::min<int>(g->num_sms * 8,
+                                (int)((g->nv + 255) / 256)));
+  minprop_init<OP><<<init_grid, 256, 0, st>>>(a, nw_alloc);
+  THV_CUDA(cudaGetLastError());
+  void *args[] = {&a};
+  THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(grid),
+                                       dim3(kMinThreads), args, smem, st));
+  launches += 2;
+  return THV_OK;
+}
+
+thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
+                       cudaStream_t st, thv_stats *stats) {
+  const int op = algo == THV_ALGO_BFS ? OP_BFS : algo == THV_ALGO_CC ? OP_CC : OP_SSSP;
+  if (op == OP_SSSP && !g->weighted)
+    return fail(THV_EINVAL, "SSSP needs edge weights (WCSR, or CSR opened "
+                            "with THV_OPEN_WEIGHTS)");
+  if (g->fmt == THV_FMT_CSC)
+    return fail(THV_EINVAL, "BFS/CC/SSSP need out-edges (CSR/WCSR), got CSC");
+  if (g->nv >= 0xFFFFFFFFull)
+    return fail(THV_EUNSUPPORTED, "vertex count %llu exceeds u32 values",
+                (unsigned long long)g->nv);
+  const uint32_t src = o ? o->source : 1;
+  if (op != OP_CC && src >= g->nv)
+    return fail(THV_EINVAL, "source %u out of range (n=%llu)", src,
+                (unsigned long long)g->nv);
+  uint32_t chunk = o && o->chunk_edges ? o->chunk_edges : kDefaultChunk;
+  chunk = std::max<uint32_t>(32, (chunk + 31) / 32 * 32);
+  const uint32_t small = o && o->small_degree ? o->small_degree : kDefaultSmall;
+  THV_TRY(ensure_plan(g));
+  THV_TRY(ensure_min_state(g, chunk, small));
+  MinState *ms = g->ms;
+
+  MinArgs a{};
+  a.val = ms->d_val;
+  a.bm = ms->d_bm;
+  a.off = g->d_off;
+  a.blk_vb = g->plan.d_vbegin;
+  a.blk_base = g->plan.d_base;
+  a.host_base = g->h_edges_dev;
+  a.qs = ms->d_qs;
+  a.qb = ms->d_qb;
+  a.cap_s = ms->cap_s;
+  a.cap_b = ms->cap_b;
+  a.ctrl = ms->d_ctrl;
+  const uint32_t tmo = o && o->timeout_ms ? o->timeout_ms : 60000u;
+  a.timeout_ns = (unsigned long long)tmo * 1000000ull;
+  a.nblk = (uint32_t)g->plan.blocks.size();
+  a.nv = (uint32_t)g->nv;
+  a.ngroups = ms->ngroups;
+  a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0xFFFFFFF0ull) * 2 + 8;
+  a.delta = o && o->sssp_delta ? o->sssp_delta : 64u;
+  a.small_deg = small;
+  a.chunk = chunk;
+  a.src = src;
+
+  uint32_t launches = 0;
+  THV_CUDA(cudaEventRecord(ms->ev0, st));
+  thv_status s = THV_OK;
+  if (g->esz == 4) {
+    if (op == OP_BFS) s = launch_minprop<OP_BFS, 4>(g, a, st, launches);
+    else if (op == OP_CC) s = launch_minprop<OP_CC, 4>(g, a, st, launches);
+    else s = fail(THV_EINVAL, "SSSP needs 8-byte weighted edges");
+  } else {
+    if (op == OP_BFS) s = launch_minprop<OP_BFS, 8>(g, a, st, launches);
+    else if (op == OP_CC) s = launch_minprop<OP_CC, 8>(g, a, st, launches);
+    else s = launch_minprop<OP_SSSP, 8>(g, a, st, launches);
+  }
+  if (s != THV_OK) return s;
+  THV_CUDA(cudaEventRecord(ms->ev1, st));
+  THV_CUDA(cudaMemcpyAsync(ms->h_ctrl, ms->d_ctrl, sizeof(MinCtrl),
+                           cudaMemcpyDeviceToHost, st));
+  THV_CUDA(cudaStreamSynchronize(st));
+  const MinCtrl &hc = *ms->h_ctrl;
+  g->last_algo = algo;
+  if (stats) {
+    float ms_ = 0.f;
+    cudaEventElapsedTime(&ms_, ms->ev0, ms->ev1);
+    stats->device_ms = ms_;
+    stats->iterations = hc.iters;
+    stats->edges_expanded = hc.edges;
+    stats->hbm_edge_bytes = hc.hbm_bytes;
+    stats->link_edge_bytes = hc.link_bytes;
+    stats->kernel_launches = launches;
+    stats->d2h_bytes += sizeof(MinCtrl);
+  }
+  if (hc.err == kDevErrBarrier)
+    return fail(THV_ETIMEOUT, "grid barrier wait exceeded %u ms", tmo);
+  if (hc.err == kDevErrIters)
+    return fail(THV_ETIMEOUT, "iteration cap %u reached", a.max_iters);
+  if (hc.err == kDevErrQueue)
+    return fail(THV_EDEVICE, "work queue overflow");
+  if (hc.err) return fail(THV_EDEVICE, "device error %u", hc.err);
+  return THV_OK;
+}
+
+thv_status minprop_values(thv_graph *g, uint32_t *out, cudaStream_t st) {
+  if (!g->ms || !g->ms->valid) return fail(THV_EINVAL, "no values: nothing ran");
+  THV_CUDA(cudaMemcpyAsync(out, g->ms->d_val, g->nv * 4, cudaMemcpyDeviceToHost, st));
+  THV_CUDA(cudaStreamSynchronize(st));
+  return THV_OK;
+}
+
+const uint32_t *minprop_device_values(thv_graph *g) {
+  return g->ms ? g->ms->d_val : nullptr;
+}
+
+}  // namespace thv

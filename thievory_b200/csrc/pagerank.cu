@@ -1,0 +1,415 @@
+// PageRank, pull (CSC in-edges) and push (CSR out-edges).
+//
+// Method (fixed by the engine's contract, not the reference's): FP32 ranks,
+// damping d, a fixed iteration count, dangling mass spread uniformly:
+//     r'(v) = (1-d)/N + d * ( sum_{u->v} r(u)/outdeg(u) + D/N ),
+//     D = sum of r(u) over vertices with outdeg(u) = 0,   r0 = 1/N.
+// The reference's kernels this replaces are src/pr/pr_kernels.cu:23-160
+// (pull: static/demand/filter) with PR32_Update_Values :449-476, and
+// :504-681 (push) with PR32_Update_Values_PUSH :846-860; those iterate to a
+// 1e-3 tolerance in FP64 without dangling redistribution.
+//
+// Every iteration streams all edges.  A CTA takes one tile (<= 4096 edges of
+// consecutive vertices inside one edge block), stages the tile's adjacency in
+// shared memory with 16-byte vector loads -- full 128-byte lines whether the
+// block is in HBM or read zero-copy from pinned host memory -- and then
+// gathers (pull) or scatters (push) per edge.  Per-vertex sums are FP64
+// (warp segmented reductions); stored ranks and contributions are FP32.
+// Pull fuses the rank update into the gather: a vertex's sum is complete
+// inside its tile, except high-degree vertices cut into parts, whose last
+// part (atomic counter) finishes the update.
+#include <algorithm>
+
+#include "thv_device.cuh"
+#include "thv_internal.h"
+
+namespace thv {
+
+constexpr int kPrThreads = 256;
+constexpr int kPrWarps = kPrThreads / 32;
+constexpr int kStageEdges = 4096;  // == kTileEdges of the tiler
+
+struct PrArgs {
+  const PrTile *tiles;
+  const uint64_t *blk_base;
+  const uint64_t *off;
+  const uint32_t *outdeg;  // CSC: explicit; CSR: nullptr (from offsets)
+  const float *cur;
+  float *nxt;
+  float *rank;
+  double *sum;
+  double *split_acc;
+  uint32_t *split_done;
+  const uint32_t *split_parts;
+  double *dang;
+  uint32_t *tile_ctr;
+  uint32_t ntiles, nv, it, pad;
+  double damping, inv_n;
+};
+
+struct PrState {
+  uint64_t nv = 0;
+  uint32_t iters = 0;
+  float *d_c[2] = {nullptr, nullptr};
+  float *d_rank = nullptr;
+  double *d_sum = nullptr;
+  double *d_split_acc = nullptr;
+  uint32_t *d_split_done = nullptr;
+  double *d_dang = nullptr;
+  uint32_t *d_tile_ctr = nullptr;
+  uint32_t cap_iters = 0;
+  size_t nsplit = 0;
+  bool push = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+__device__ __forceinline__ uint32_t out_degree(const PrArgs &a, uint32_t v) {
+  return a.outdeg ? __ldg(a.outdeg + v)
+                  : (uint32_t)(__ldg(a.off + v + 1) - __ldg(a.off + v));
+}
+
+__device__ __forceinline__ double finish_vertex(const PrArgs &a, uint32_t v,
+                                                double sum, double base) {
+  const double r = base + a.damping * sum;
+  a.rank[v] = (float)r;
+  const uint32_t od = out_degree(a, v);
+  a.nxt[v] = od ? (float)(r / (double)od) : 0.f;
+  return od ? 0.0 : r;
+}
+
+template <int ESZ>
+__device__ __forceinline__ uint32_t staged_id(const uint32_t *s_e, uint32_t i) {
+  return s_e[(size_t)i * (ESZ / 4)];
+}
+
+// Stage edges [t.ebegin, t.eend) of a tile; returns the element shift.
+template <int ESZ>
+__device__ __forceinline__ uint32_t stage_tile(const PrArgs &a, const PrTile &t,
+                                               uint32_t *s_e) {
+  const uintptr_t b = (uintptr_t)__ldg(a.blk_base + t.block);
+  const uintptr_t s0 = b + (uintptr_t)t.ebegin * ESZ;
+  const uintptr_t s1 = b + (uintptr_t)t.eend * ESZ;
+  const uintptr_t a0 = s0 & ~(uintptr_t)15;
+  const uint32_t nvec = (uint32_t)((s1 - a0 + 15) / 16);
+  uint4 *dst = reinterpret_cast<uint4 *>(s_e);
+  for (uint32_t i = threadIdx.x; i < nvec; i += blockDim.x) dst[i] = ld_nc_v4(a0 + 16u * i);
+  return (uint32_t)((s0 - a0) / ESZ);
+}
+
+__device__ __forceinline__ double block_sum(double x, double *s_red) {
+  x = warp_sum(x);
+  const unsigned w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) s_red[w] = x;
+  __syncthreads();
+  double t = 0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (unsigned)kPrWarps ? s_red[threadIdx.x] : 0.0;
+    t = warp_sum(t);
+  }
+  __syncthreads();
+  return t;  // valid in thread 0..31
+}
+
+template <int ESZ>
+__global__ void __launch_bounds__(kPrThreads) pr_pull_kernel(PrArgs a) {
+  __shared__ __align__(16) uint32_t s_e[kStageEdges * (ESZ / 4) + 16];
+  __shared__ double s_acc[kPrWarps][32];
+  __shared__ double s_red[kPrWarps];
+  __shared__ uint32_t s_tile;
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  const double base = (1.0 - a.damping) * a.inv_n + a.damping * ldcg(a.dang + a.it) * a.inv_n;
+  double dsum = 0.0;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr + a.it, 1u);
+    __syncthreads();
+    const uint32_t ti = s_tile;
+    if (ti >= a.ntiles) break;
+    const PrTile t = a.tiles[ti];
+    const uint32_t shift = stage_tile<ESZ>(a, t, s_e);
+    __syncthreads();
+    if (t.split) {
+      const uint32_t cnt = (uint32_t)(t.eend - t.ebegin);
+      double part = 0.0;
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+        part += (double)__ldg(a.cur + staged_id<ESZ>(s_e, shift + i));
+      part = block_sum(part, s_red);
+      if (threadIdx.x == 0) {
+        const uint32_t s = t.split - 1;
+        atomicAdd(a.split_acc + s, part);
+        __threadfence();
+        const uint32_t done = atomicAdd(a.split_done + s, 1u);
+        if (done + 1 == __ldg(a.split_parts + s)) {
+          __threadfence();
+          const unsigned long long bits =
+              atomicExch(reinterpret_cast<unsigned long long *>(a.split_acc + s), 0ull);
+          a.split_done[s] = 0;
+          dsum += finish_vertex(a, t.vbegin, __longlong_as_double((long long)bits), base);
+        }
+      }
+    } else {
+      const uint32_t nverts = t.vend - t.vbegin;
+      const uint32_t ngroups = (nverts + 31) / 32;
+      for (uint32_t g = warp; g < ngroups; g += kPrWarps) {
+        const uint32_t v = t.vbegin + g * 32 + lane;
+        const bool valid = v < t.vend;
+        uint32_t ls = 0, deg = 0;
+        if (valid) {
+          const uint64_t e0 = __ldg(a.off + v), e1 = __ldg(a.off + v + 1);
+          ls = (uint32_t)(e0 - t.ebegin);
+          deg = (uint32_t)(e1 - e0);
+        }
+        const unsigned incl = warp_incl_scan<unsigned>(deg);
+        const unsigned excl = incl - deg;
+        const unsigned total = __shfl_sync(kFull, incl, 31);
+        s_acc[warp][lane] = 0.0;
+        __syncwarp();
+        for (unsigned k = 0; k < total; k += 32) {
+          const unsigned tt = k + lane;
+          const int o = warp_owner(excl, tt);
+          const unsigned ols = __shfl_sync(kFull, ls, o);
+          const unsigned oex = __shfl_sync(kFull, excl, o);
+          double x = 0.0;
+          int pos = 32;
+          if (tt < total) {
+            x = (double)__ldg(a.cur + staged_id<ESZ>(s_e, shift + ols + (tt - oex)));
+            pos = o;
+          }
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const double y = __shfl_up_sync(kFull, x, d);
+            const int pp = __shfl_up_sync(kFull, pos, d);
+            if (lane >= (unsigned)d && pp == pos) x += y;
+          }
+          const int nxt = __shfl_down_sync(kFull, pos, 1);
+          if ((lane == 31 || nxt != pos) && pos < 32) s_acc[warp][pos] += x;
+          __syncwarp();
+        }
+        if (valid) dsum += finish_vertex(a, v, s_acc[warp][lane], base);
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+  }
+  dsum = block_sum(dsum, s_red);
+  if (threadIdx.x == 0 && dsum != 0.0) atomicAdd(a.dang + a.it + 1, dsum);
+}
+
+template <int ESZ>
+__global__ void __launch_bounds__(kPrThreads) pr_push_kernel(PrArgs a) {
+  __shared__ __align__(16) uint32_t s_e[kStageEdges * (ESZ / 4) + 16];
+  __shared__ uint32_t s_tile;
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(a.tile_ctr + a.it, 1u);
+    __syncthreads();
+    const uint32_t ti = s_tile;
+    if (ti >= a.ntiles) break;
+    const PrTile t = a.tiles[ti];
+    const uint32_t shift = stage_tile<ESZ>(a, t, s_e);
+    __syncthreads();
+    if (t.split) {
+      const double c = (double)__ldg(a.cur + t.vbegin);
+      const uint32_t cnt = (uint32_t)(t.eend - t.ebegin);
+      for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+        atomicAdd(a.sum + staged_id<ESZ>(s_e, shift + i), c);
+    } else {
+      const uint32_t nverts = t.vend - t.vbegin;
+      const uint32_t ngroups = (nverts + 31) / 32;
+      for (uint32_t g = warp; g < ngroups; g += kPrWarps) {
+        const uint32_t u = t.vbegin + g * 32 + lane;
+        uint32_t ls = 0, deg = 0;
+        float c = 0.f;
+        if (u < t.vend) {
+          const uint64_t e0 = __ldg(a.off + u), e1 = __ldg(a.off + u + 1);
+          ls = (uint32_t)(e0 - t.ebegin);
+          deg = (uint32_t)(e1 - e0);
+          c = __ldg(a.cur + u);
+        }
+        const unsigned incl = warp_incl_scan<unsigned>(deg);
+        const unsigned excl = incl - deg;
+        const unsigned total = __shfl_sync(kFull, incl, 31);
+        for (unsigned k = 0; k < total; k += 32) {
+          const unsigned tt = k + lane;
+          const int o = warp_owner(excl, tt);
+          const unsigned ols = __shfl_sync(kFull, ls, o);
+          const unsigned oex = __shfl_sync(kFull, excl, o);
+          const float oc = __shfl_sync(kFull, c, o);
+          if (tt < total)
+            atomicAdd(a.sum + staged_id<ESZ>(s_e, shift + ols + (tt - oex)), (double)oc);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void pr_push_update(PrArgs a) {
+  __shared__ double s_red[kPrWarps];
+  const double base = (1.0 - a.damping) * a.inv_n + a.damping * ldcg(a.dang + a.it) * a.inv_n;
+  double dsum = 0.0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nv; v += gridDim.x * blockDim.x) {
+    const double s = a.sum[v];
+    a.sum[v] = 0.0;
+    dsum += finish_vertex(a, v, s, base);
+  }
+  dsum = block_sum(dsum, s_red);
+  if (threadIdx.x == 0 && dsum != 0.0) atomicAdd(a.dang + a.it + 1, dsum);
+}
+
+__global__ void pr_init(PrArgs a, float *c0) {
+  __shared__ double s_red[kPrWarps];
+  double dsum = 0.0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nv; v += gridDim.x * blockDim.x) {
+    a.rank[v] = (float)a.inv_n;
+    const uint32_t od = out_degree(a, v);
+    c0[v] = od ? (float)(a.inv_n / (double)od) : 0.f;
+    if (!od) dsum += a.inv_n;
+    if (a.sum) a.sum[v] = 0.0;
+  }
+  dsum = block_sum(dsum, s_red);
+  if (threadIdx.x == 0 && dsum != 0.0) atomicAdd(a.dang, dsum);
+}
+
+// ------------------------------------------------------------------ host --
+
+void pagerank_free(thv_graph *g) {
+  PrState *p = g->ps;
+  if (!p) return;
+  dev_free(p->d_c[0]);
+  dev_free(p->d_c[1]);
+  dev_free(p->d_rank);
+  dev_free(p->d_sum);
+  dev_free(p->d_split_acc);
+  dev_free(p->d_split_done);
+  dev_free(p->d_dang);
+  dev_free(p->d_tile_ctr);
+  if (p->ev0) cudaEventDestroy(p->ev0);
+  if (p->ev1) cudaEventDestroy(p->ev1);
+  delete p;
+  g->ps = nullptr;
+}
+
+static thv_status ensure_pr_state(thv_graph *g, bool push, uint32_t iters) {
+  PrState *&p = g->ps;
+  const size_t nsplit = std::max<size_t>(1, g->plan.split_parts.size());
+  if (p && p->push == push && p->cap_iters >= iters && p->nsplit == nsplit) return THV_OK;
+  pagerank_free(g);
+  p = new PrState();
+  p->nv = g->nv;
+  p->push = push;
+  p->nsplit = nsplit;
+  p->cap_iters = std::max<uint32_t>(iters, 32);
+  THV_TRY(dev_alloc((void **)&p->d_c[0], g->nv * 4 + 64, "pr contributions"));
+  THV_TRY(dev_alloc((void **)&p->d_c[1], g->nv * 4 + 64, "pr contributions"));
+  THV_TRY(dev_alloc((void **)&p->d_rank, g->nv * 4 + 64, "pr ranks"));
+  if (push) THV_TRY(dev_alloc((void **)&p->d_sum, g->nv * 8 + 64, "pr sums"));
+  THV_TRY(dev_alloc((void **)&p->d_split_acc, nsplit * 8, "pr split sums"));
+  THV_TRY(dev_alloc((void **)&p->d_split_done, nsplit * 4, "pr split counters"));
+  THV_TRY(dev_alloc((void **)&p->d_dang, (p->cap_iters + 1) * 8, "pr dangling"));
+  THV_TRY(dev_alloc((void **)&p->d_tile_ctr, p->cap_iters * 4, "pr tile counters"));
+  THV_CUDA(cudaEventCreate(&p->ev0));
+  THV_CUDA(cudaEventCreate(&p->ev1));
+  return THV_OK;
+}
+
+template <int ESZ>
+static thv_status pr_iterate(thv_graph *g, PrArgs &a, bool push, uint32_t iters,
+                             cudaStream_t st, uint32_t &launches) {
+  PrState *p = g->ps;
+  int bpsm = 0;
+  if (push)
+    THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, pr_push_kernel<ESZ>, kPrThreads, 0));
+  else
+    THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, pr_pull_kernel<ESZ>, kPrThreads, 0));
+  const int grid = std::max(1, bpsm) * g->num_sms;
+  const int ugrid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + kPrThreads - 1) / kPrThreads)));
+  for (uint32_t it = 0; it < iters; it++) {
+    a.it = it;
+    a.cur = p->d_c[it & 1];
+    a.nxt = p->d_c[(it + 1) & 1];
+    if (push) {
+      pr_push_kernel<ESZ><<<grid, kPrThreads, 0, st>>>(a);
+      pr_push_update<<<ugrid, kPrThreads, 0, st>>>(a);
+      launches += 2;
+    } else {
+      pr_pull_kernel<ESZ><<<grid, kPrThreads, 0, st>>>(a);
+      launches += 1;
+    }
+    THV_CUDA(cudaGetLastError());
+  }
+  return THV_OK;
+}
+
+thv_status run_pagerank(thv_graph *g, thv_algo algo, const thv_run_opts *o,
+                        cudaStream_t st, thv_stats *stats) {
+  const bool push = algo == THV_ALGO_PR_PUSH;
+  if (push && g->fmt == THV_FMT_CSC)
+    return fail(THV_EINVAL, "push PageRank needs out-edges (CSR), got CSC");
+  if (!push && g->fmt != THV_FMT_CSC)
+    return fail(THV_EINVAL, "pull PageRank needs in-edges (CSC)");
+  if (g->nv == 0) return fail(THV_EINVAL, "empty graph");
+  const uint32_t iters = o && o->pr_iters ? o->pr_iters : 20u;
+  const double damping = o && o->pr_damping > 0 ? o->pr_damping : 0.85;
+  THV_TRY(ensure_plan(g));
+  THV_TRY(build_tiles(g));
+  THV_TRY(ensure_pr_state(g, push, iters));
+  PrState *p = g->ps;
+  p->iters = iters;
+
+  PrArgs a{};
+  a.tiles = g->plan.d_tiles;
+  a.blk_base = g->plan.d_base;
+  a.off = g->d_off;
+  a.outdeg = g->fmt == THV_FMT_CSC ? g->d_outdeg : nullptr;
+  a.rank = p->d_rank;
+  a.sum = p->d_sum;
+  a.split_acc = p->d_split_acc;
+  a.split_done = p->d_split_done;
+  a.split_parts = g->plan.d_split_parts;
+  a.dang = p->d_dang;
+  a.tile_ctr = p->d_tile_ctr;
+  a.ntiles = (uint32_t)g->plan.tiles.size();
+  a.nv = (uint32_t)g->nv;
+  a.damping = damping;
+  a.inv_n = 1.0 / (double)g->nv;
+
+  uint32_t launches = 0;
+  THV_CUDA(cudaEventRecord(p->ev0, st));
+  THV_CUDA(cudaMemsetAsync(p->d_dang, 0, (iters + 1) * 8, st));
+  THV_CUDA(cudaMemsetAsync(p->d_tile_ctr, 0, iters * 4, st));
+  const size_t nsplit = std::max<size_t>(1, g->plan.split_parts.size());
+  THV_CUDA(cudaMemsetAsync(p->d_split_acc, 0, nsplit * 8, st));
+  THV_CUDA(cudaMemsetAsync(p->d_split_done, 0, nsplit * 4, st));
+  const int ugrid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + kPrThreads - 1) / kPrThreads)));
+  pr_init<<<ugrid, kPrThreads, 0, st>>>(a, p->d_c[0]);
+  THV_CUDA(cudaGetLastError());
+  launches++;
+  thv_status s = g->esz == 8 ? pr_iterate<8>(g, a, push, iters, st, launches)
+                             : pr_iterate<4>(g, a, push, iters, st, launches);
+  if (s != THV_OK) return s;
+  THV_CUDA(cudaEventRecord(p->ev1, st));
+  THV_CUDA(cudaStreamSynchronize(st));
+  g->last_algo = algo;
+  if (stats) {
+    float ms_ = 0.f;
+    cudaEventElapsedTime(&ms_, p->ev0, p->ev1);
+    stats->device_ms = ms_;
+    stats->iterations = iters;
+    stats->edges_expanded = g->ne * iters;
+    stats->hbm_edge_bytes = g->plan.tiles_hbm_bytes * iters;
+    stats->link_edge_bytes = g->plan.tiles_link_bytes * iters;
+    stats->kernel_launches = launches;
+  }
+  return THV_OK;
+}
+
+thv_status pagerank_values(thv_graph *g, double *out, cudaStream_t st) {
+  if (!g->ps) return fail(THV_EINVAL, "no PageRank values");
+  std::vector<float> tmp(g->nv);
+  THV_CUDA(cudaMemcpyAsync(tmp.data(), g->ps->d_rank, g->nv * 4, cudaMemcpyDeviceToHost, st));
+  THV_CUDA(cudaStreamSynchronize(st));
+  for (uint64_t i = 0; i < g->nv; i++) out[i] = (double)tmp[i];
+  return THV_OK;
+}
+
+}  // namespace thv

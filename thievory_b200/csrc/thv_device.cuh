@@ -1,0 +1,130 @@
+// Device-side helpers: coherent loads, warp collectives, bounded grid barrier.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace thv {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+// Device error codes written into a control word (0 = ok).
+enum : unsigned {
+  kDevOk = 0,
+  kDevErrBarrier = 1,   // a grid barrier wait ran out of time
+  kDevErrIters = 2,     // iteration cap reached
+  kDevErrQueue = 3,     // work queue capacity exceeded
+  kDevErrDepth = 4,     // batched BFS level exceeded the u8 range
+};
+
+// L2-coherent load (bypasses the non-coherent L1) for data other SMs write.
+__device__ __forceinline__ uint32_t ldcg(const uint32_t *p) { return __ldcg(p); }
+__device__ __forceinline__ unsigned long long ldcg(const unsigned long long *p) {
+  return __ldcg(p);
+}
+__device__ __forceinline__ double ldcg(const double *p) { return __ldcg(p); }
+
+// Read-only 16-byte load; works for HBM and for host-mapped pinned memory.
+__device__ __forceinline__ uint4 ld_nc_v4(uintptr_t addr) {
+  return __ldg(reinterpret_cast<const uint4 *>(addr));
+}
+__device__ __forceinline__ uint32_t ld_nc_u32(uintptr_t addr) {
+  return __ldg(reinterpret_cast<const uint32_t *>(addr));
+}
+__device__ __forceinline__ uint2 ld_nc_u2(uintptr_t addr) {
+  return __ldg(reinterpret_cast<const uint2 *>(addr));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_incl_scan(T x) {
+  const unsigned lane = lane_id();
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    T y = __shfl_up_sync(kFull, x, d);
+    if (lane >= (unsigned)d) x += y;
+  }
+  return x;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x += __shfl_xor_sync(kFull, x, d);
+  return x;
+}
+
+__device__ __forceinline__ unsigned warp_min(unsigned x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x = min(x, __shfl_xor_sync(kFull, x, d));
+  return x;
+}
+
+__device__ __forceinline__ unsigned long long shfl64(unsigned long long x,
+                                                     int src) {
+  return __shfl_sync(kFull, x, src);
+}
+
+// Largest lane l with excl[l] <= t, for excl non-decreasing across the warp.
+__device__ __forceinline__ int warp_owner(unsigned excl, unsigned t) {
+  int pos = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const unsigned e = __shfl_sync(kFull, excl, pos + s);
+    if (e <= t) pos += s;
+  }
+  return pos;
+}
+
+// Grid-wide barrier for a cooperative launch.  The wait is bounded by
+// timeout_ns of %globaltimer; on expiry the error word is set and every
+// block leaves through the false return.  Returns false if any block has
+// flagged an error.
+struct GridBar {
+  unsigned count;
+  unsigned gen;
+};
+
+__device__ __forceinline__ bool grid_sync(GridBar *bar, unsigned *err,
+                                          unsigned long long timeout_ns) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned gen = *((volatile unsigned *)&bar->gen);
+    __threadfence();
+    const unsigned arrived = atomicAdd(&bar->count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      const unsigned long long t0 = global_ns();
+      unsigned spins = 0;
+      while (*((volatile unsigned *)&bar->gen) == gen) {
+        if ((++spins & 63u) == 0 && global_ns() - t0 > timeout_ns) {
+          atomicCAS(err, 0u, kDevErrBarrier);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *((volatile unsigned *)err) == 0;
+}
+
+}  // namespace thv

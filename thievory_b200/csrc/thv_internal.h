@@ -1,0 +1,139 @@
+// Internal host-side definitions shared by the engine's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "thv.h"
+
+namespace thv {
+
+// Thread-local error message; returns the status for `return fail(...)`.
+thv_status fail(thv_status s, const char *fmt, ...);
+bool alloc_should_fail();  // host fault-injection hook
+
+#define THV_CUDA(call)                                                      \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      return ::thv::fail(THV_ECUDA, "%s:%d %s: %s", __FILE__, __LINE__,     \
+                         #call, cudaGetErrorString(e_));                    \
+  } while (0)
+
+#define THV_TRY(expr)                          \
+  do {                                         \
+    thv_status s_ = (expr);                    \
+    if (s_ != THV_OK) return s_;               \
+  } while (0)
+
+// Device allocation with the fault-injection hook.
+thv_status dev_alloc(void **p, size_t bytes, const char *what);
+thv_status pinned_alloc(void **p, size_t bytes, const char *what);
+void dev_free(void *p);
+void pinned_free(void *p);
+
+// Edge block: a vertex range whose adjacency is contiguous in the edge array.
+struct Block {
+  uint32_t vbegin, vend;
+  uint64_t ebegin, eend;  // edge indices
+  bool resident;
+  uint64_t dev_elem;      // element offset inside the resident buffer
+};
+
+// Dense-iteration tile (PageRank): a vertex range with <= kTileEdges edges
+// inside one block, or one part of a high-degree vertex ("split" tile).
+struct __align__(16) PrTile {
+  uint64_t ebegin, eend;
+  uint32_t vbegin, vend;
+  uint32_t block;
+  uint32_t split;  // 0, or 1 + index of the split vertex
+};
+
+struct Plan {
+  bool valid = false;
+  uint64_t budget_bytes = 0, block_bytes = 0;
+  uint32_t policy = 0;
+  std::vector<Block> blocks;
+  std::vector<uint32_t> vbegin;     // nb+1 entries
+  std::vector<uint64_t> base;       // per-block virtual base address
+  char *d_resident = nullptr;       // packed resident blocks
+  size_t d_resident_bytes = 0;
+  uint32_t *d_vbegin = nullptr;
+  uint64_t *d_base = nullptr;
+  uint64_t resident_edge_bytes = 0, host_edge_bytes = 0;
+  // PageRank tiles (built lazily)
+  bool tiles_valid = false;
+  std::vector<PrTile> tiles;
+  std::vector<uint32_t> split_parts;  // per split vertex
+  PrTile *d_tiles = nullptr;
+  uint32_t *d_split_parts = nullptr;
+  uint64_t tiles_hbm_bytes = 0, tiles_link_bytes = 0;
+};
+
+struct MinState;  // minprop.cu
+struct PrState;   // pagerank.cu
+struct BatchState;  // batch.cu
+
+}  // namespace thv
+
+struct thv_graph {
+  uint64_t nv = 0, ne = 0;
+  thv_format fmt = THV_FMT_CSR;
+  uint32_t esz = 4;
+  bool weighted = false;
+  int device = 0;
+  // host
+  std::vector<uint64_t> off;      // nv+1
+  void *h_edges = nullptr;        // pinned + mapped, padded
+  size_t h_edges_bytes = 0;
+  uint64_t h_edges_dev = 0;       // device address of h_edges
+  std::vector<uint32_t> outdeg;   // CSC only
+  // device
+  cudaStream_t stream = nullptr;
+  uint64_t *d_off = nullptr;
+  uint32_t *d_outdeg = nullptr;   // CSC only
+  int num_sms = 0;
+  thv::Plan plan;
+  thv::MinState *ms = nullptr;
+  thv::PrState *ps = nullptr;
+  thv::BatchState *bs = nullptr;
+  // last run
+  int last_algo = -1;
+  size_t device_bytes = 0;
+};
+
+namespace thv {
+
+constexpr uint64_t kDefaultBlockBytes = 64ull << 20;  // reference PARTITION_SIZE_MB
+constexpr size_t kEdgePad = 1024;                     // bytes of slack past arrays
+
+thv_status graph_init_device(thv_graph *g);  // stream, d_off, d_outdeg
+thv_status ensure_plan(thv_graph *g);
+thv_status build_tiles(thv_graph *g);
+void plan_free(thv_graph *g);
+
+thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
+                       cudaStream_t st, thv_stats *stats);
+thv_status minprop_values(thv_graph *g, uint32_t *out, cudaStream_t st);
+const uint32_t *minprop_device_values(thv_graph *g);
+void minprop_free(thv_graph *g);
+
+thv_status run_pagerank(thv_graph *g, thv_algo algo, const thv_run_opts *o,
+                        cudaStream_t st, thv_stats *stats);
+thv_status pagerank_values(thv_graph *g, double *out, cudaStream_t st);
+void pagerank_free(thv_graph *g);
+
+thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
+                     uint32_t n, const thv_batch_opts *o, uint32_t *out,
+                     thv_stats *stats);
+void batch_free(thv_graph *g);
+
+thv_status generate_rmat(const thv_rmat_opts *o, thv_format fmt, int device,
+                         thv_graph **out);
+
+double now_ms();
+
+}  // namespace thv
