@@ -83,6 +83,11 @@ int main(int argc, char **argv) {
     if (edge == 4 && type == "push") PR32_PUSH(path, runs, 0, numa);
     else PR32(path, runs, 0, numa);
   }
+  // the reference checks no launch; report the context's state after the run
+  const cudaError_t sync = cudaDeviceSynchronize();
+  const cudaError_t last = cudaGetLastError();
+  printf("Post-run CUDA status: sync=%s last=%s\n", cudaGetErrorString(sync),
+         cudaGetErrorString(last));
   if (ballast) cudaFree(ballast);
-  return 0;
+  return sync == cudaSuccess && last == cudaSuccess ? 0 : 2;
 }

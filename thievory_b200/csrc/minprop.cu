@@ -24,7 +24,10 @@
 // bit-exact whatever the schedule: BFS level+1, CC min reaching id, SSSP
 // min(dist+1, n+1).  SSSP takes only pending vertices below a moving
 // threshold (near/far split) to avoid re-expanding vertices whose distance
-// is still falling.
+// is still falling -- each re-expansion of a non-resident vertex re-reads
+// its adjacency over the host link.  A per-bitmap-word lower bound of the
+// pending values lets the compaction skip words that hold only far
+// vertices without reading their values.
 //
 // Each vertex's adjacency is addressed through its edge block's base
 // address: resident blocks point into the HBM buffer, the others into the
@@ -44,6 +47,8 @@ constexpr int kMinThreads = 512;
 constexpr uint32_t kSmemBlocks = 2048;  // block table kept in shared memory
 constexpr uint32_t kDefaultSmall = 64;  // degree < this: warp-cooperative
 constexpr uint32_t kDefaultChunk = 256; // edges per high-degree work item
+constexpr uint32_t kDefaultDelta = 2;   // SSSP near/far width (weights >= 1)
+constexpr uint32_t kCcGrowth = 8;       // CC label window growth per advance
 
 struct __align__(16) WorkItem {
   uint64_t eaddr;  // address of the first edge (device or host-mapped)
@@ -62,6 +67,7 @@ struct MinCtrl {
 struct MinArgs {
   uint32_t *val;
   uint32_t *bm;
+  uint32_t *wmin;  // SSSP: lower bound of the pending values in each bitmap word
   const uint64_t *off;
   const uint32_t *blk_vb;
   const uint64_t *blk_base;
@@ -72,12 +78,14 @@ struct MinArgs {
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, max_iters;
   uint32_t delta, small_deg, chunk, src;
+  uint32_t growth, pad;
 };
 
 struct MinState {
   uint64_t nv = 0;
   uint32_t *d_val = nullptr;
   uint32_t *d_bm = nullptr;
+  uint32_t *d_wmin = nullptr;
   WorkItem *d_qs = nullptr, *d_qb = nullptr;
   uint64_t cap_s = 0, cap_b = 0;
   uint32_t chunk = 0, small = 0;
@@ -99,65 +107,78 @@ __device__ __forceinline__ uint32_t find_block(const uint32_t *vb, uint32_t nblk
   return lo;
 }
 
-__device__ __forceinline__ void relax(const MinArgs &a, uint32_t w,
-                                      unsigned long long cand) {
-  uint32_t *vp = a.val + w;
-  if (cand < ldcg(vp)) {
-    const uint32_t old = atomicMin(vp, (uint32_t)cand);
-    if (cand < old) {
-      const uint32_t m = 1u << (w & 31u);
-      uint32_t *bp = a.bm + (w >> 5);
-      if (!(ldcg(bp) & m)) atomicOr(bp, m);
+template <int OP>
+__device__ __forceinline__ void activate(const MinArgs &a, uint32_t w,
+                                         unsigned long long cand) {
+  if (OP != OP_BFS) atomicMin(a.wmin + (w >> 5), (uint32_t)cand);
+  const uint32_t m = 1u << (w & 31u);
+  uint32_t *bp = a.bm + (w >> 5);
+  if (!(ldcg(bp) & m)) atomicOr(bp, m);
+}
+
+// Relax N edges at once: all value probes are issued before any atomic so a
+// lane keeps N loads in flight.
+template <int OP, int N>
+__device__ __forceinline__ void relax_n(const MinArgs &a, const uint32_t (&w)[N],
+                                        const unsigned long long (&cand)[N],
+                                        const bool (&ok)[N]) {
+  uint32_t cur[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) cur[j] = ok[j] ? ldcg(a.val + w[j]) : 0u;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    if (ok[j] && cand[j] < cur[j]) {
+      const uint32_t old = atomicMin(a.val + w[j], (uint32_t)cand[j]);
+      if (cand[j] < old) activate<OP>(a, w[j], cand[j]);
     }
   }
 }
 
-template <int OP, int ESZ>
-__device__ __forceinline__ void relax_vec(const MinArgs &a, uint4 q,
-                                          uintptr_t p, uintptr_t start,
-                                          uintptr_t end, uint32_t vval) {
-  if (ESZ == 4) {
-    const uint32_t e[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const uintptr_t ea = p + 4u * j;
-      if (ea >= start && ea < end) {
-        const unsigned long long cand =
-            OP == OP_BFS ? (unsigned long long)vval + 1ull : vval;
-        relax(a, e[j], cand);
-      }
-    }
-  } else {
-    const uint32_t d[2] = {q.x, q.z}, wt[2] = {q.y, q.w};
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      const uintptr_t ea = p + 8u * j;
-      if (ea >= start && ea < end) {
-        const unsigned long long cand =
-            OP == OP_BFS    ? (unsigned long long)vval + 1ull
-            : OP == OP_SSSP ? (unsigned long long)vval + wt[j]
-                            : (unsigned long long)vval;
-        relax(a, d[j], cand);
-      }
-    }
-  }
+template <int OP>
+__device__ __forceinline__ unsigned long long candidate(uint32_t vval, uint32_t wt) {
+  return OP == OP_BFS    ? (unsigned long long)vval + 1ull
+         : OP == OP_SSSP ? (unsigned long long)vval + wt
+                         : (unsigned long long)vval;
 }
 
+// One high-degree chunk per warp: 128-byte aligned 16-byte loads, two per
+// lane in flight, lanes outside [start, end) masked.
 template <int OP, int ESZ>
-__device__ void process_chunk(const MinArgs &a, const WorkItem &it) {
+__device__ __forceinline__ void process_chunk(const MinArgs &a, const WorkItem &it) {
+  constexpr int PER = 16 / ESZ;  // edges per 16-byte load
   const unsigned lane = lane_id();
   const uint32_t vval = ldcg(a.val + it.v);
   const uintptr_t start = it.eaddr;
   const uintptr_t end = start + (uintptr_t)it.cnt * ESZ;
-  for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end;
-       p += 512u) {
-    const uint4 q = ld_nc_v4(p);
-    relax_vec<OP, ESZ>(a, q, p, start, end, vval);
+  for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end; p += 1024u) {
+    uint4 q[2];
+    q[0] = ld_nc_v4(p);
+    const bool second = p + 512u < end;
+    q[1] = second ? ld_nc_v4(p + 512u) : make_uint4(0, 0, 0, 0);
+    uint32_t w[2 * PER];
+    unsigned long long cand[2 * PER];
+    bool ok[2 * PER];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const uintptr_t ph = p + 512u * h;
+      const uint32_t f[4] = {q[h].x, q[h].y, q[h].z, q[h].w};
+#pragma unroll
+      for (int j = 0; j < PER; j++) {
+        const uintptr_t ea = ph + (uintptr_t)ESZ * j;
+        const int k = h * PER + j;
+        ok[k] = (h == 0 || second) && ea >= start && ea < end;
+        w[k] = ESZ == 4 ? f[j] : f[2 * j];
+        cand[k] = candidate<OP>(vval, ESZ == 4 ? 0u : f[2 * j + 1]);
+      }
+    }
+    relax_n<OP, 2 * PER>(a, w, cand, ok);
   }
 }
 
+// 32 low-degree vertices per warp: warp-cooperative load balancing over
+// their concatenated adjacency, 64 edges per step (two per lane in flight).
 template <int OP, int ESZ>
-__device__ void process_group(const MinArgs &a, unsigned long long first,
+__device__ __forceinline__ void process_group(const MinArgs &a, unsigned long long first,
                               unsigned long long n_small) {
   const unsigned lane = lane_id();
   const unsigned long long idx = first + lane;
@@ -170,28 +191,36 @@ __device__ void process_group(const MinArgs &a, unsigned long long first,
   const unsigned incl = warp_incl_scan<unsigned>(it.cnt);
   const unsigned excl = incl - it.cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
-  for (unsigned k = 0; k < total; k += 32) {
-    const unsigned t = k + lane;
-    const int o = warp_owner(excl, t);
-    const unsigned long long ea = shfl64(it.eaddr, o);
-    const unsigned oex = __shfl_sync(kFull, excl, o);
-    const uint32_t ov = __shfl_sync(kFull, vval, o);
-    if (t < total) {
-      const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
+  for (unsigned k = 0; k < total; k += 64) {
+    uint32_t w[2];
+    unsigned long long cand[2];
+    bool ok[2];
+    uintptr_t addr[2];
+    uint32_t ov[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const unsigned t = k + 32u * h + lane;
+      const int o = warp_owner(excl, t);
+      const unsigned long long ea = shfl64(it.eaddr, o);
+      const unsigned oex = __shfl_sync(kFull, excl, o);
+      ov[h] = __shfl_sync(kFull, vval, o);
+      ok[h] = t < total;
+      addr[h] = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
+    }
+    uint32_t wt[2] = {0, 0};
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
       if (ESZ == 4) {
-        const uint32_t w = ld_nc_u32(addr);
-        const unsigned long long cand =
-            OP == OP_BFS ? (unsigned long long)ov + 1ull : ov;
-        relax(a, w, cand);
+        w[h] = ok[h] ? ld_nc_u32(addr[h]) : 0u;
       } else {
-        const uint2 e = ld_nc_u2(addr);
-        const unsigned long long cand =
-            OP == OP_BFS    ? (unsigned long long)ov + 1ull
-            : OP == OP_SSSP ? (unsigned long long)ov + e.y
-                            : (unsigned long long)ov;
-        relax(a, e.x, cand);
+        const uint2 e = ok[h] ? ld_nc_u2(addr[h]) : make_uint2(0, 0);
+        w[h] = e.x;
+        wt[h] = e.y;
       }
     }
+#pragma unroll
+    for (int h = 0; h < 2; h++) cand[h] = candidate<OP>(ov[h], wt[h]);
+    relax_n<OP, 2>(a, w, cand, ok);
   }
 }
 
@@ -211,8 +240,14 @@ __global__ void __launch_bounds__(kMinThreads)
   const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
 
+  // Only pending vertices with value < thr are expanded.  SSSP: a window of
+  // fixed width above the smallest pending distance.  CC: labels in
+  // increasing order, the window growing geometrically each time it empties,
+  // so each component's minimum label floods it in one wave.
   uint32_t thr = 0xFFFFFFFFu;
+  uint32_t width = a.delta;
   if (OP == OP_SSSP) thr = (uint32_t)min(1ull + a.delta, 0xFFFFFFFFull);
+  if (OP == OP_CC) thr = a.delta;
 
   unsigned iter = 0;
   for (;; ++iter) {
@@ -236,6 +271,16 @@ __global__ void __launch_bounds__(kMinThreads)
       const unsigned wbase = g * 32u;
       const uint32_t word = ldcg(a.bm + wbase + lane);
       unsigned nz = __ballot_sync(kFull, word != 0);
+      if (OP != OP_BFS) {
+        // a word whose pending values are all >= thr is kept without
+        // touching its vertices
+        const uint32_t wm = word ? ldcg(a.wmin + wbase + lane) : 0xFFFFFFFFu;
+        if (word != 0 && wm >= thr) {
+          my_keep += __popc(word);
+          my_min = min(my_min, wm);
+        }
+        nz = __ballot_sync(kFull, word != 0 && wm < thr);
+      }
       while (nz) {
         const int j = __ffs(nz) - 1;
         nz &= nz - 1;
@@ -244,15 +289,19 @@ __global__ void __launch_bounds__(kMinThreads)
         const bool act = (wd >> lane) & 1u;
         bool take = act;
         uint32_t vval = 0;
-        if (OP == OP_SSSP && act) {
+        if (OP != OP_BFS && act) {
           vval = ldcg(a.val + v);
           take = vval < thr;
         }
         const unsigned tm = __ballot_sync(kFull, take);
-        if (OP == OP_SSSP) {
+        if (OP != OP_BFS) {
           const bool kept = act && !take;
-          my_min = min(my_min, kept ? vval : 0xFFFFFFFFu);
-          if (lane == 0) my_keep += __popc(wd & ~tm);
+          const uint32_t kmin = warp_min(kept ? vval : 0xFFFFFFFFu);
+          my_min = min(my_min, kmin);
+          if (lane == 0) {
+            my_keep += __popc(wd & ~tm);
+            a.wmin[wbase + j] = kmin;
+          }
         }
         if (lane == 0 && tm) a.bm[wbase + j] = wd & ~tm;
         uint32_t deg = 0;
@@ -308,14 +357,17 @@ __global__ void __launch_bounds__(kMinThreads)
     my_hbm = warp_sum(my_hbm);
     my_link = warp_sum(my_link);
     my_verts = warp_sum(my_verts);
-    if (OP == OP_SSSP) my_min = warp_min(my_min);
+    if (OP != OP_BFS) {
+      my_min = warp_min(my_min);
+      my_keep = warp_sum(my_keep);
+    }
     if (lane == 0 && my_verts) {
       atomicAdd(&c->edges, my_edges);
       atomicAdd(&c->hbm_bytes, my_hbm);
       atomicAdd(&c->link_bytes, my_link);
       atomicAdd(&c->vertices, my_verts);
     }
-    if (OP == OP_SSSP && lane == 0) {
+    if (OP != OP_BFS && lane == 0) {
       if (my_keep) atomicAdd(&c->remaining[slot], my_keep);
       if (my_min != 0xFFFFFFFFu) atomicMin(&c->minkept[slot], my_min);
     }
@@ -324,10 +376,11 @@ __global__ void __launch_bounds__(kMinThreads)
     const unsigned long long ns = ldcg(&c->cnt_small[slot]);
     const unsigned long long nb = ldcg(&c->cnt_big[slot]);
     if (ns + nb == 0) {
-      if (OP != OP_SSSP) break;
+      if (OP == OP_BFS) break;
       if (ldcg(&c->remaining[slot]) == 0) break;
       const uint32_t mk = ldcg(&c->minkept[slot]);
-      thr = (uint32_t)min((unsigned long long)mk + a.delta, 0xFFFFFFFFull);
+      if (OP == OP_CC) width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
+      thr = (uint32_t)min((unsigned long long)mk + width, 0xFFFFFFFFull);
       continue;
     }
     // ----------------------------------------------------------- expansion
@@ -358,13 +411,21 @@ __global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
   for (uint64_t w = tid; w < nw_alloc; w += stride) {
     uint32_t word = 0;
     if (OP == OP_CC) {
+      // every vertex with out-edges is pending with its own id as label
       const uint64_t lo = w * 32ull;
-      if (lo + 32 <= a.nv) word = 0xFFFFFFFFu;
-      else if (lo < a.nv) word = (1u << (a.nv - lo)) - 1u;
+      const uint64_t hi = lo + 32ull < (uint64_t)a.nv ? lo + 32ull : (uint64_t)a.nv;
+      uint64_t prev = lo < hi ? a.off[lo] : 0;
+      for (uint64_t v = lo; v < hi; v++) {
+        const uint64_t nx = a.off[v + 1];
+        if (nx > prev) word |= 1u << (v - lo);
+        prev = nx;
+      }
+      a.wmin[w] = lo < 0xFFFFFFFFull ? (uint32_t)lo : 0xFFFFFFFFu;
     } else if (w == (a.src >> 5)) {
       word = 1u << (a.src & 31u);
     }
     a.bm[w] = word;
+    if (OP == OP_SSSP) a.wmin[w] = w == (a.src >> 5) ? 1u : 0xFFFFFFFFu;
   }
   if (tid == 0) {
     MinCtrl *c = a.ctrl;
@@ -392,6 +453,7 @@ static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
   ms->cap_b = g->ne / chunk + g->ne / std::max<uint32_t>(small, 1) + 64;
   THV_TRY(dev_alloc((void **)&ms->d_val, g->nv * 4 + 64, "values"));
   THV_TRY(dev_alloc((void **)&ms->d_bm, nw_alloc * 4, "pending bitmap"));
+  THV_TRY(dev_alloc((void **)&ms->d_wmin, nw_alloc * 4, "pending minima"));
   THV_TRY(dev_alloc((void **)&ms->d_qs, ms->cap_s * sizeof(WorkItem), "queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(WorkItem), "chunk queue"));
   THV_TRY(dev_alloc((void **)&ms->d_ctrl, sizeof(MinCtrl), "control"));
@@ -407,6 +469,7 @@ void minprop_free(thv_graph *g) {
   if (!ms) return;
   dev_free(ms->d_val);
   dev_free(ms->d_bm);
+  dev_free(ms->d_wmin);
   dev_free(ms->d_qs);
   dev_free(ms->d_qb);
   dev_free(ms->d_ctrl);
@@ -465,6 +528,7 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   MinArgs a{};
   a.val = ms->d_val;
   a.bm = ms->d_bm;
+  a.wmin = ms->d_wmin;
   a.off = g->d_off;
   a.blk_vb = g->plan.d_vbegin;
   a.blk_base = g->plan.d_base;
@@ -480,7 +544,8 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.nv = (uint32_t)g->nv;
   a.ngroups = ms->ngroups;
   a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0xFFFFFFF0ull) * 2 + 8;
-  a.delta = o && o->sssp_delta ? o->sssp_delta : 64u;
+  a.delta = o && o->sssp_delta ? o->sssp_delta : (op == OP_CC ? 1u : kDefaultDelta);
+  a.growth = kCcGrowth;
   a.small_deg = small;
   a.chunk = chunk;
   a.src = src;
