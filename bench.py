@@ -38,6 +38,26 @@ SEED = 0x54484592
 FALLBACK_HBM_GBS = 6650.0
 
 
+# DRAM and host-link (sysmem) bytes per launch of the dominant kernel, from the
+# ncu captures summarised in profiles/ (minprop_sssp_rmat22_wcsr_hbm40.md,
+# minprop_bfs_rmat20_resident.md, pr_pull_rmat22_csc_hbm47.md).  Captures
+# made on a smaller graph are scaled to the bench size by edge count (the
+# traffic of these kernels grows with the edges traversed).
+NCU_TRAFFIC = {
+    "sssp": dict(scale=22, ne=65241959, dram=298979072 + 14398464, sysmem=11397242 * 32),
+    "bfs": dict(scale=20, ne=16084564, dram=78297088 + 4716544, sysmem=0),
+    "pr_pull": dict(scale=22, ne=65241959, dram=135399168 + 20317184, sysmem=6104134 * 32, per="iteration"),
+}
+
+
+def traffic_for(algo, scale, ne, iters=1):
+    t = NCU_TRAFFIC.get(algo)
+    if not t:
+        return None, None
+    f = ne / t["ne"]
+    return int(t["dram"] * f * iters), int(t["sysmem"] * f * iters)
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -54,6 +74,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
     ap.add_argument("--scale", type=int, default=0, help="override the workload's scale")
+    ap.add_argument("--source", type=int, default=1, help="BFS/SSSP source vertex")
+    ap.add_argument("--budget-frac", type=float, default=-1.0,
+                    help="override the HBM edge budget as a fraction of edge bytes")
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -187,7 +210,9 @@ def run_ours(args, dist):
     wl = dict(WORKLOADS[args.workload])
     if args.scale:
         wl["scale"] = args.scale
-    result = {}
+    if args.budget_frac >= 0:
+        wl.pop("budget", None)
+        wl["frac"] = args.budget_frac
 
     link_mc, link_zc = T.link_bandwidth(dev, 1 << 30)
     link_peak = max(link_mc, link_zc)
@@ -200,7 +225,7 @@ def run_ours(args, dist):
         budget = wl.get("budget", int(wl.get("frac", 1.0) * g.ne * g.esz))
         plan = g.plan(budget)
         algo = wl["algo"]
-        src = 1
+        src = args.source
         sptr = stream.cuda_stream
         for _ in range(w):
             g.run(algo, source=src, want_values=False, stream=sptr)
@@ -237,6 +262,7 @@ def run_ours(args, dist):
         value = dist.n * trav * k / total_s / 1e9
         t_roof = b_hbm / (hbm_peak * 1e9) + b_link / (link_peak * 1e9)
         kern_s = statistics.mean(lib_ms) / 1e3
+        dram_t, link_t = traffic_for(algo, wl["scale"], g.ne, iters)
         out = {
             "value": value, "ms_per_step": total_s * 1e3 / k, "traversed_edges": trav,
             "plan": plan, "clocks": ck, "gpu_launches": launches,
@@ -245,7 +271,9 @@ def run_ours(args, dist):
                 "achieved": (b_hbm + b_link) / kern_s / 1e9,
                 "peak": (b_hbm + b_link) / t_roof / 1e9,
                 "frac": t_roof / kern_s,
-                "traffic": None,
+                "traffic": dram_t, "link_traffic": link_t,
+                "traffic_note": "dram read+write (and host-link sysmem sectors) per launch from an "
+                                "ncu capture, scaled by edge count when captured on a smaller graph",
                 "algorithmic_hbm_bytes": b_hbm, "algorithmic_link_bytes": b_link,
                 "hbm_peak_gbs": hbm_peak, "hbm_peak_kind": peak_kind,
                 "link_peak_gbs": link_peak, "link_memcpy_gbs": link_mc, "link_zerocopy_gbs": link_zc,
@@ -312,7 +340,8 @@ def run_reference(args, dist):
         wl["scale"] = args.scale
     g = O.rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"], weighted=wl["algo"] == "sssp")
     algo = wl["algo"]
-    fn = {"sssp": lambda: O.sssp(g, 1, parallel=True), "bfs": lambda: O.bfs(g, 1, parallel=True),
+    fn = {"sssp": lambda: O.sssp(g, args.source, parallel=True),
+          "bfs": lambda: O.bfs(g, args.source, parallel=True),
           "cc": lambda: O.cc(g, parallel=True),
           "pr_pull": lambda: O.pagerank(g, 20)}[algo]
     for _ in range(args.warmup):
@@ -358,7 +387,7 @@ def main():
             "config": {"workload": f"{wl['algo']} rmat{wl['scale']} ef{wl['ef']} {wl['fmt']} "
                                    f"hbm-budget {budget_desc}",
                        "scale": wl["scale"], "edge_factor": wl["ef"], "format": wl["fmt"],
-                       "hbm_edge_budget": budget_desc, "source": 1,
+                       "hbm_edge_budget": budget_desc, "source": args.source,
                        "resident_edge_bytes": m["plan"]["resident_edge_bytes"],
                        "host_edge_bytes": m["plan"]["host_edge_bytes"],
                        "traversed_edges_per_step": m["traversed_edges"],

@@ -180,15 +180,18 @@ typedef struct thv_batch_opts {
   uint32_t group;        /* sources per group, 1..64; 0 = 64 */
   uint32_t timeout_ms;   /* 0 = 60000 */
   void *stream;
-  uint32_t tuned;        /* 1 = use the autotuner's choice (default) */
-  uint32_t pad;
+  uint32_t small_degree; /* expansion tuning; 0 = autotuned / default */
+  uint32_t chunk_edges;  /* expansion tuning; 0 = autotuned / default */
 } thv_batch_opts;
 
-/* out: n x nv u32 values, row i = result for sources[i], in the plain
- * encoding (bit-exact equal to thv_run of that source). */
+/* Runs n sources in groups sharing one traversal each.  out (host, may be
+ * NULL): n x nv u32, row i = values for sources[i] in the single-source
+ * encoding, bit-exact equal to thv_run of that source.  checksums (may be
+ * NULL): per source, sum over v of splitmix64((v << 32) | value) mod 2^64,
+ * so results too large to copy can still be compared with single runs. */
 thv_status thv_batch_run(thv_graph *g, thv_algo algo, const uint32_t *sources,
                          uint32_t n, const thv_batch_opts *o, uint32_t *out,
-                         thv_stats *stats);
+                         uint64_t *checksums, thv_stats *stats);
 
 /* ---- serving (continuous batching) ---- */
 typedef struct thv_server thv_server;

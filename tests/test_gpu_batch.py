@@ -1,0 +1,90 @@
+"""Batched multi-source BFS / SSSP: every per-source result equals the
+single-source run bit for bit (values and the per-source checksum)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+BLOCK = 64 << 10
+
+
+@pytest.fixture(scope="module")
+def g14(O):
+    return O.rmat(14, 16)
+
+
+@pytest.fixture(scope="module")
+def g14w(O, g14):
+    return O.CSR(g14.off, g14.adj, O.weights(g14))
+
+
+def sources(O, g, n):
+    s = O.sources(g, n).tolist()
+    s[0] = 1               # may be isolated: a trivial query in the mix
+    s[-1] = s[1]           # duplicate source inside a group
+    return np.array(s, np.uint32)
+
+
+@pytest.mark.parametrize("frac,group", [(0.0, 64), (0.4, 64), (1.0, 64), (0.4, 7), (0.4, 1)])
+def test_batched_bfs_equals_single(T, O, g14, frac, group):
+    src = sources(O, g14, 70)
+    with T.Graph.from_arrays(g14.off, g14.adj, "csr") as g:
+        g.plan(int(frac * g.ne * 4), block_bytes=BLOCK)
+        out, sums, st = g.batch_run("bfs", src, group=group, timeout_ms=20000)
+        for i, s in enumerate(src):
+            want = O.bfs(g14, int(s))
+            assert np.array_equal(out[i], want), f"source {s}"
+            assert int(sums[i]) == T.values_checksum(want)
+        assert st["iterations"] > 0
+
+
+@pytest.mark.parametrize("frac", [0.0, 0.4, 1.0])
+def test_batched_sssp_equals_single(T, O, g14w, frac):
+    src = sources(O, g14w, 66)
+    with T.Graph.from_arrays(g14w.off, g14w.wcsr_edges(), "wcsr") as g:
+        g.plan(int(frac * g.ne * 8), block_bytes=BLOCK)
+        out, sums, _ = g.batch_run("sssp", src, timeout_ms=20000)
+        for i, s in enumerate(src):
+            want = O.sssp(g14w, int(s))
+            assert np.array_equal(out[i], want), f"source {s}"
+            assert int(sums[i]) == T.values_checksum(want)
+
+
+def test_batched_checksums_only(T, O, g14w):
+    src = sources(O, g14w, 64)
+    with T.Graph.from_arrays(g14w.off, g14w.wcsr_edges(), "wcsr") as g:
+        g.plan(int(0.4 * g.ne * 8), block_bytes=BLOCK)
+        out, sums, _ = g.batch_run("bfs", src, want_values=False)
+        assert out is None
+        for i, s in enumerate(src[:8]):
+            vals, _ = g.run("bfs", source=int(s))
+            assert int(sums[i]) == T.values_checksum(vals)
+
+
+def test_batched_tuning_is_result_neutral(T, O, g14):
+    src = sources(O, g14, 64)
+    with T.Graph.from_arrays(g14.off, g14.adj, "csr") as g:
+        g.plan(int(0.4 * g.ne * 4), block_bytes=BLOCK)
+        a, sa, _ = g.batch_run("bfs", src)
+        b, sb, _ = g.batch_run("bfs", src, small_degree=8, chunk_edges=64)
+        assert np.array_equal(a, b) and np.array_equal(sa, sb)
+
+
+def test_deep_graph_falls_back_to_single_runs(T, O):
+    n = 300  # a path deeper than the 254 levels a level byte holds
+    c = O.from_edges(n, np.arange(n - 1), np.arange(1, n))
+    with T.Graph.from_arrays(c.off, c.adj, "csr") as g:
+        g.plan()
+        out, sums, _ = g.batch_run("bfs", [0, 5, 299], timeout_ms=20000)
+        for i, s in enumerate([0, 5, 299]):
+            assert np.array_equal(out[i], O.bfs(c, s))
+
+
+def test_batch_rejects_bad_input(T, O, g14):
+    with T.Graph.from_arrays(g14.off, g14.adj, "csr") as g:
+        with pytest.raises(T.ThvError):
+            g.batch_run("bfs", [g14.nv])
+        with pytest.raises(T.ThvError):
+            g.batch_run("sssp", [1])  # no weights
+        with pytest.raises(T.ThvError):
+            g.batch_run("cc", [1])

@@ -87,7 +87,8 @@ class _RmatOpts(ctypes.Structure):
 
 class _BatchOpts(ctypes.Structure):
     _fields_ = [("group", ctypes.c_uint32), ("timeout_ms", ctypes.c_uint32),
-                ("stream", ctypes.c_void_p), ("tuned", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+                ("stream", ctypes.c_void_p), ("small_degree", ctypes.c_uint32),
+                ("chunk_edges", ctypes.c_uint32)]
 
 
 class _ServeOpts(ctypes.Structure):
@@ -144,7 +145,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_run": ([P, U32, ctypes.POINTER(_RunOpts), P, ctypes.POINTER(_Stats)], I32),
         "thv_values": ([P, P], I32),
         "thv_write_values": ([ctypes.c_char_p, P, U64, U32], I32),
-        "thv_batch_run": ([P, U32, P, U32, ctypes.POINTER(_BatchOpts), P, ctypes.POINTER(_Stats)], I32),
+        "thv_batch_run": ([P, U32, P, U32, ctypes.POINTER(_BatchOpts), P, P,
+                           ctypes.POINTER(_Stats)], I32),
         "thv_serve_start": ([P, ctypes.POINTER(_ServeOpts), pp], I32),
         "thv_serve_submit": ([P, U32, U32, ctypes.POINTER(ctypes.c_uint64)], I32),
         "thv_serve_poll": ([P, U64, P, ctypes.POINTER(_QueryStats)], I32),
@@ -272,15 +274,20 @@ class Graph:
         return buf
 
     def batch_run(self, algo: str, sources: Sequence[int], group: int = 64,
-                  stream: int = 0, tuned: bool = True):
+                  want_values: bool = True, stream: int = 0, small_degree: int = 0,
+                  chunk_edges: int = 0, timeout_ms: int = 0):
+        """Batched BFS/SSSP; returns (values [n, nv] or None, checksums [n], stats)."""
         lib = load_library()
         src = np.ascontiguousarray(sources, dtype=np.uint32)
-        out = np.empty((len(src), self.nv), dtype=np.uint32)
-        o = _BatchOpts(group, 0, ctypes.c_void_p(stream) if stream else None, 1 if tuned else 0, 0)
+        out = np.empty((len(src), self.nv), dtype=np.uint32) if want_values else None
+        sums = np.empty(len(src), dtype=np.uint64)
+        o = _BatchOpts(group, timeout_ms, ctypes.c_void_p(stream) if stream else None,
+                       small_degree, chunk_edges)
         st = _Stats()
         _check(lib.thv_batch_run(self._h, ALGO[algo], _ptr(src), len(src), ctypes.byref(o),
-                                 _ptr(out), ctypes.byref(st)), f"thv_batch_run({algo})")
-        return out, st.to_dict()
+                                 None if out is None else _ptr(out), _ptr(sums),
+                                 ctypes.byref(st)), f"thv_batch_run({algo})")
+        return out, sums, st.to_dict()
 
     def save(self, path: str) -> None:
         _check(load_library().thv_save(self._h, path.encode()), "thv_save")
@@ -413,6 +420,19 @@ def PR32_PUSH(file_path: str, n_runs: int = 1, n_neighbor_gpus: int = 0,
               hbm_budget_bytes: Optional[int] = None, values_path: str = "results/values.bin"):
     return _driver(file_path, "csr", False, "pr_push", 0, n_runs, n_neighbor_gpus,
                    hbm_budget_bytes, values_path)
+
+
+def values_checksum(values: np.ndarray) -> int:
+    """Order-independent checksum of a u32 value array, as thv_batch_run
+    computes per source: sum over v of splitmix64((v << 32) | value) mod 2^64."""
+    v = np.asarray(values, dtype=np.uint64)
+    x = (np.arange(len(v), dtype=np.uint64) << np.uint64(32)) | v
+    with np.errstate(over="ignore"):
+        x = x + np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        x = x ^ (x >> np.uint64(31))
+        return int(x.sum(dtype=np.uint64))
 
 
 def link_bandwidth(device: int = 0, nbytes: int = 1 << 30):

@@ -673,11 +673,11 @@ thv_status thv_write_values(const char *path, const void *values, uint64_t n,
 
 thv_status thv_batch_run(thv_graph *g, thv_algo algo, const uint32_t *sources,
                          uint32_t n, const thv_batch_opts *o, uint32_t *out,
-                         thv_stats *stats) {
+                         uint64_t *checksums, thv_stats *stats) {
   THV_GUARD_BEGIN
   if (!g || (!sources && n)) return fail(THV_EINVAL, "null argument");
   THV_CUDA(cudaSetDevice(g->device));
-  return run_batch(g, algo, sources, n, o, out, stats);
+  return run_batch(g, algo, sources, n, o, out, checksums, stats);
   THV_GUARD_END
 }
 

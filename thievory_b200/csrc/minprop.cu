@@ -44,17 +44,11 @@ namespace thv {
 enum { OP_BFS = 0, OP_CC = 1, OP_SSSP = 2 };
 
 constexpr int kMinThreads = 512;
-constexpr uint32_t kSmemBlocks = 2048;  // block table kept in shared memory
 constexpr uint32_t kDefaultSmall = 64;  // degree < this: warp-cooperative
 constexpr uint32_t kDefaultChunk = 256; // edges per high-degree work item
 constexpr uint32_t kDefaultDelta = 2;   // SSSP near/far width (weights >= 1)
 constexpr uint32_t kCcGrowth = 8;       // CC label window growth per advance
 
-struct __align__(16) WorkItem {
-  uint64_t eaddr;  // address of the first edge (device or host-mapped)
-  uint32_t v;
-  uint32_t cnt;
-};
 
 struct MinCtrl {
   GridBar bar;
@@ -95,17 +89,6 @@ struct MinState {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool valid = false;
 };
-
-__device__ __forceinline__ uint32_t find_block(const uint32_t *vb, uint32_t nblk,
-                                               uint32_t v) {
-  uint32_t lo = 0, hi = nblk;
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (vb[mid] <= v) lo = mid;
-    else hi = mid;
-  }
-  return lo;
-}
 
 template <int OP>
 __device__ __forceinline__ void activate(const MinArgs &a, uint32_t w,
@@ -384,18 +367,20 @@ __global__ void __launch_bounds__(kMinThreads)
       continue;
     }
     // ----------------------------------------------------------- expansion
+    // task ids: chunks first, then groups of 32 small vertices; each warp
+    // starts on task gwarp, then draws from a shared counter (no atomic at
+    // all for warps without a first task)
     const unsigned long long ntask = nb + (ns + 31) / 32;
-    for (;;) {
-      unsigned long long t = 0;
-      if (lane == 0) t = atomicAdd(&c->wc[slot], 1ull);
-      t = shfl64(t, 0);
-      if (t >= ntask) break;
+    for (unsigned long long t = gwarp; t < ntask;) {
       if (t < nb) {
         const WorkItem it = a.qb[t];
         process_chunk<OP, ESZ>(a, it);
       } else {
         process_group<OP, ESZ>(a, (t - nb) * 32ull, ns);
       }
+      unsigned long long nt = 0;
+      if (lane == 0) nt = nwarps + atomicAdd(&c->wc[slot], 1ull);
+      t = shfl64(nt, 0);
     }
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
   }

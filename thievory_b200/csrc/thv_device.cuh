@@ -89,6 +89,28 @@ __device__ __forceinline__ int warp_owner(unsigned excl, unsigned t) {
   return pos;
 }
 
+// Frontier work item: the adjacency of vertex v (or one chunk of it) at a
+// device or host-mapped address.
+struct __align__(16) WorkItem {
+  uint64_t eaddr;
+  uint32_t v;
+  uint32_t cnt;
+};
+
+constexpr uint32_t kSmemBlocks = 2048;  // block tables up to this size go to smem
+
+// Edge block of vertex v: largest b with vb[b] <= v (vb has nblk+1 entries).
+__device__ __forceinline__ uint32_t find_block(const uint32_t *vb, uint32_t nblk,
+                                               uint32_t v) {
+  uint32_t lo = 0, hi = nblk;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (vb[mid] <= v) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // Grid-wide barrier for a cooperative launch.  The wait is bounded by
 // timeout_ns of %globaltimer; on expiry the error word is set and every
 // block leaves through the false return.  Returns false if any block has

@@ -128,7 +128,7 @@ void pagerank_free(thv_graph *g);
 
 thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
                      uint32_t n, const thv_batch_opts *o, uint32_t *out,
-                     thv_stats *stats);
+                     uint64_t *checksums, thv_stats *stats);
 void batch_free(thv_graph *g);
 
 thv_status generate_rmat(const thv_rmat_opts *o, thv_format fmt, int device,
