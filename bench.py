@@ -72,7 +72,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--edge-factor", type=int, default=0, help="override the edge factor")
+    ap.add_argument("--rates", default="", help="c5: comma-separated arrival rates (queries/s)")
+    ap.add_argument("--queries", type=int, default=1024, help="c4: batched sources")
+    ap.add_argument("--plain-sample", type=int, default=16, help="c4: single-source runs timed")
     ap.add_argument("--scale", type=int, default=0, help="override the workload's scale")
     ap.add_argument("--source", type=int, default=1, help="BFS/SSSP source vertex")
     ap.add_argument("--budget-frac", type=float, default=-1.0,
@@ -331,6 +335,104 @@ def run_ours(args, dist):
     return wl, main, extra
 
 
+def run_batched(args, dist):
+    """Config 4: 1,024 seeded sources over the non-isolated vertices, batched
+    in groups of 64 (one persistent launch per group) vs single-source runs
+    of a sample of the same sources; per-source checksums of the sample must
+    match the batched ones bit for bit."""
+    import torch
+    import thievory_b200 as T
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    T.load_library()
+    scale = args.scale or 26
+    budget = 2 << 30 if args.budget_frac < 0 else None
+    out = {}
+    for algo, fmt in (("bfs", "csr"), ("sssp", "wcsr")):
+        g = T.Graph.generate_rmat(scale, 16, seed=SEED, fmt=fmt, device=dev)
+        g.plan(budget if budget is not None else int(args.budget_frac * g.ne * g.esz))
+        src = g.pick_sources(args.queries, SEED)
+        g.batch_run(algo, src[:64], want_values=False)  # warm-up
+        _, sums, bst = g.batch_run(algo, src, want_values=False)
+        plain_ms = []
+        for s_ in src[: args.plain_sample]:
+            vals, st = g.run(algo, source=int(s_))
+            plain_ms.append(st["device_ms"])
+            i = int(np.nonzero(src == s_)[0][0])
+            assert T.values_checksum(vals) == int(sums[i]), f"{algo} source {s_} differs"
+        qps_b = dist.n * len(src) / (dist.max(bst["device_ms"]) / 1e3)
+        qps_p = dist.n * 1e3 / dist.max(statistics.mean(plain_ms))
+        out[algo] = {"batched_qps": qps_b, "plain_qps": qps_p, "speedup": qps_b / qps_p,
+                     "batched_ms_total": bst["device_ms"], "plain_ms_mean": statistics.mean(plain_ms),
+                     "queries": len(src), "plain_sample": args.plain_sample,
+                     "batched_link_bytes": bst["link_edge_bytes"], "batched_iterations": bst["iterations"],
+                     "checked": f"{args.plain_sample} sources: single-run checksum == batched checksum"}
+        g.close()
+    return scale, out
+
+
+def run_serving(args, dist):
+    """Config 5 (scaled to the box): a Poisson stream, 80% BFS / 20% SSSP,
+    sources uniform over non-isolated vertices, served by continuous batching
+    vs the same stream run one query at a time with the plain kernels (FIFO
+    replay of measured single-query device times on the same arrivals).
+    Every served query's checksum must equal its plain run's."""
+    import torch
+    import thievory_b200 as T
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    T.load_library()
+    scale = args.scale or 26
+    ef = args.edge_factor or 48
+    frac = args.budget_frac if args.budget_frac >= 0 else 0.58
+    g = T.Graph.generate_rmat(scale, ef, seed=SEED, fmt="wcsr", device=dev)
+    plan = g.plan(int(frac * g.ne * g.esz))
+    n = args.queries
+    src = g.pick_sources(n, SEED)
+    algos = ["sssp" if i % 5 == 0 else "bfs" for i in range(n)]
+    plain_ms, plain_sum = [], []
+    for a, s_ in zip(algos, src):
+        _, st = g.run(a, source=int(s_), want_values=False, checksum=True)
+        plain_ms.append(st["device_ms"])
+        plain_sum.append(st["checksum"])
+    rng = np.random.default_rng(SEED)
+    rates = [float(x) for x in args.rates.split(",")] if args.rates else [
+        0.5 * 1e3 / statistics.mean(plain_ms), 4e3 / statistics.mean(plain_ms),
+        32e3 / statistics.mean(plain_ms)]
+    sweep = []
+    for rate in rates:
+        arr = np.cumsum(rng.exponential(1.0 / rate, n))
+        # plain: FIFO replay of the measured service times on these arrivals
+        fin, lat = 0.0, []
+        for t_a, ms in zip(arr, plain_ms):
+            fin = max(fin, t_a) + ms / 1e3
+            lat.append(fin - t_a)
+        plain_qps = n / (fin - arr[0])
+        with T.Server(g, max_slots=64) as sv:
+            t0 = time.perf_counter()
+            tickets = []
+            for i, (a, s_) in enumerate(zip(algos, src)):
+                d = t0 + arr[i] - arr[0] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets.append(sv.submit(a, int(s_), want_values=False))
+            stats = [sv.wait(t, timeout_ms=600000)[1] for t in tickets]
+            t1 = time.perf_counter()
+        for i, st in enumerate(stats):
+            assert st["checksum"] == plain_sum[i], f"query {i} ({algos[i]} {src[i]}) differs"
+        slat = np.array([st["latency_ms"] for st in stats])
+        sweep.append({"rate_qps": rate, "served_qps": n / (t1 - t0),
+                      "served_p50_ms": float(np.percentile(slat, 50)),
+                      "served_p99_ms": float(np.percentile(slat, 99)),
+                      "plain_qps": plain_qps,
+                      "plain_p50_ms": float(np.percentile(np.array(lat) * 1e3, 50)),
+                      "plain_p99_ms": float(np.percentile(np.array(lat) * 1e3, 99))})
+    g.close()
+    return scale, ef, frac, plan, sweep, statistics.mean(plain_ms)
+
+
 def run_reference(args, dist):
     """CPU oracle (the reference has no CPU path) on the same workload."""
     from oracle import oracle as O
@@ -373,6 +475,38 @@ def main():
                                  "sample": f"full {wl['algo']} run per step on the host (OpenMP oracle)"},
                 "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        dist.close()
+        return
+    if args.workload == "c5":
+        scale, ef, frac, plan, sweep, plain_mean = run_serving(args, dist)
+        if dist.rank == 0:
+            top = max(sweep, key=lambda r: r["served_qps"])
+            line = {"metric": "queries/s served (continuous batching, 80% BFS / 20% SSSP)",
+                    "value": top["served_qps"], "unit": "queries/s", "n_gpus": args.gpus,
+                    "steps": args.queries, "warmup": 0, "ms_per_step": 1e3 / top["served_qps"],
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                    "data": "synthetic (seeded RMAT, Poisson arrivals)",
+                    "config": {"workload": f"c5 serving rmat{scale} ef{ef} wcsr, {int(frac * 100)}% of "
+                                           f"edge bytes in HBM, {args.queries} queries per rate",
+                               "resident_edge_bytes": plan["resident_edge_bytes"],
+                               "host_edge_bytes": plan["host_edge_bytes"]},
+                    "plain_mean_ms": plain_mean, "sweep": sweep}
+            print(json.dumps(line))
+        dist.close()
+        return
+    if args.workload == "c4":
+        scale, out = run_batched(args, dist)
+        if dist.rank == 0:
+            b = out["bfs"]
+            line = {"metric": "queries/s (batched 64-source BFS)", "value": b["batched_qps"],
+                    "unit": "queries/s", "n_gpus": args.gpus, "steps": 1, "warmup": 1,
+                    "ms_per_step": b["batched_ms_total"], "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+                    "data": "synthetic (seeded RMAT)",
+                    "config": {"workload": f"c4 batched BFS/SSSP rmat{scale} ef16, 2 GiB HBM edge budget, "
+                                           f"{args.queries} seeded sources, groups of 64"},
+                    "extra": out}
+            print(json.dumps(line))
         dist.close()
         return
     wl, m, extra = run_ours(args, dist)

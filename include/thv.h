@@ -150,7 +150,13 @@ typedef struct thv_run_opts {
   void *stream;          /* cudaStream_t to launch on; NULL = graph's own */
   uint32_t small_degree; /* expansion tuning; 0 = default */
   uint32_t chunk_edges;  /* expansion tuning; 0 = default */
+  uint32_t flags;        /* THV_RUN_* */
+  uint32_t pad;
 } thv_run_opts;
+
+/* thv_run_opts.flags: also compute stats->checksum = sum over v of
+ * splitmix64((v << 32) | value) (BFS/CC/SSSP), after the timed traversal */
+#define THV_RUN_CHECKSUM 1u
 
 typedef struct thv_stats {
   double device_ms;         /* CUDA-event time of the traversal */
@@ -163,6 +169,7 @@ typedef struct thv_stats {
   uint64_t d2h_bytes;       /* explicit device->host copies in the call */
   uint32_t kernel_launches;
   uint32_t pad;
+  uint64_t checksum;        /* with THV_RUN_CHECKSUM */
 } thv_stats;
 
 /* Runs algo.  out_values (host, may be NULL) receives u32[nv] or double[nv]
@@ -182,6 +189,8 @@ typedef struct thv_batch_opts {
   void *stream;
   uint32_t small_degree; /* expansion tuning; 0 = autotuned / default */
   uint32_t chunk_edges;  /* expansion tuning; 0 = autotuned / default */
+  uint32_t sssp_delta;   /* shared near/far width for SSSP; 0 = default */
+  uint32_t pad;
 } thv_batch_opts;
 
 /* Runs n sources in groups sharing one traversal each.  out (host, may be
@@ -194,34 +203,54 @@ thv_status thv_batch_run(thv_graph *g, thv_algo algo, const uint32_t *sources,
                          uint64_t *checksums, thv_stats *stats);
 
 /* ---- serving (continuous batching) ---- */
+/* A server owns the graph while it runs (no other thv_run on it meanwhile).
+ * Queries occupy slots of one resident traversal: a query that arrives while
+ * others run is admitted at the next iteration boundary where a slot and its
+ * memory are free, and its iterations overlap theirs on the device.  Results
+ * are bit-identical to thv_run of the same source. */
 typedef struct thv_server thv_server;
 
 typedef struct thv_serve_opts {
-  uint32_t max_slots;       /* concurrent queries on the device, <= 64 */
-  uint32_t queue_capacity;  /* pending requests; 0 = 4096 */
-  uint64_t mem_budget_bytes;/* device memory for per-query state; 0 = auto */
-  uint32_t timeout_ms;
-  uint32_t pad;
+  uint32_t max_slots;        /* concurrent queries on the device, <= 64 */
+  uint32_t queue_capacity;   /* waiting requests; 0 = 65536 */
+  uint64_t mem_budget_bytes; /* device memory for per-query values (4 B per
+                                vertex per slot); 0 = all slots */
+  uint32_t timeout_ms;       /* bound on device waits; 0 = 60000 */
+  uint32_t max_batch_iters;  /* iterations per launch while requests wait;
+                                0 = 4 */
 } thv_serve_opts;
 
 typedef struct thv_query_stats {
-  double submit_to_start_ms, start_to_done_ms, latency_ms;
+  double queue_ms;   /* submit -> admitted into a slot */
+  double run_ms;     /* admitted -> result written */
+  double latency_ms; /* submit -> result written */
+  uint64_t checksum; /* sum over v of splitmix64((v << 32) | value) */
   uint32_t iterations;
   uint32_t slot;
+  int32_t status;    /* thv_status of the query */
+  uint32_t pad;
 } thv_query_stats;
 
 thv_status thv_serve_start(thv_graph *g, const thv_serve_opts *o,
                            thv_server **out);
-/* algo BFS or SSSP. Never blocks; THV_EBUSY when the queue is full. */
+/* algo BFS or SSSP.  out_values (may be NULL): nv u32 written before the
+ * ticket completes; it must stay valid until then.  Never blocks; THV_EBUSY
+ * when the waiting queue is full. */
 thv_status thv_serve_submit(thv_server *s, thv_algo algo, uint32_t source,
-                            uint64_t *ticket);
-/* THV_ENOTREADY until done; then copies u32[nv] into out (may be NULL) and
- * releases the ticket. */
-thv_status thv_serve_poll(thv_server *s, uint64_t ticket, uint32_t *out,
-                          thv_query_stats *st);
-thv_status thv_serve_wait(thv_server *s, uint64_t ticket, uint32_t *out,
-                          thv_query_stats *st, uint32_t timeout_ms);
+                            uint32_t *out_values, uint64_t *ticket);
+/* THV_ENOTREADY until the query is done; then fills st and releases the
+ * ticket. */
+thv_status thv_serve_poll(thv_server *s, uint64_t ticket, thv_query_stats *st);
+thv_status thv_serve_wait(thv_server *s, uint64_t ticket, thv_query_stats *st,
+                          uint32_t timeout_ms);
+/* Finishes every submitted query, then stops. */
 thv_status thv_serve_stop(thv_server *s);
+
+/* n sources drawn uniformly (seeded) from the vertices with out-degree > 0:
+ * draw j tries splitmix64(key ^ (j << 24 | t)) mod nv for t = 0, 1, ... with
+ * key = splitmix64(seed ^ 0x534F555243455331). */
+thv_status thv_pick_sources(const thv_graph *g, uint64_t seed, uint32_t n,
+                            uint32_t *out);
 
 /* ---- misc ---- */
 /* Host-link bandwidth of `device` in GB/s: a pinned cudaMemcpy host->device

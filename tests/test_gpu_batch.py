@@ -88,3 +88,8 @@ def test_batch_rejects_bad_input(T, O, g14):
             g.batch_run("sssp", [1])  # no weights
         with pytest.raises(T.ThvError):
             g.batch_run("cc", [1])
+
+
+def test_pick_sources_matches_oracle(T, O, g14):
+    with T.Graph.from_arrays(g14.off, g14.adj, "csr") as g:
+        assert np.array_equal(g.pick_sources(100), O.sources(g14, 100))

@@ -271,3 +271,10 @@ def test_reference_named_drivers(T, O, g14w, tmp_path, monkeypatch):
     assert np.array_equal(vals, O.cc(g14w))
     vals, _ = T.PR32_PUSH(p, 1)
     assert max_rel(vals, O.pagerank(g14w, 20)) <= PR_RTOL
+
+
+def test_run_checksum_flag(T, O, g14):
+    with engine_graph(T, g14) as g:
+        plan(g, 0.4)
+        vals, st = g.run("bfs", source=1, checksum=True)
+        assert st["checksum"] == T.values_checksum(vals)

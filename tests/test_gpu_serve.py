@@ -1,0 +1,111 @@
+"""Serving: continuous batching.  Every query's result equals the single
+-source run bit for bit, whether it ran alone or joined a traversal that
+other queries already occupied (admitted into a freed slot mid-stream)."""
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def g14w(O):
+    g = O.rmat(14, 16)
+    return O.CSR(g.off, g.adj, O.weights(g))
+
+
+@pytest.fixture(scope="module")
+def eg(T, g14w):
+    g = T.Graph.from_arrays(g14w.off, g14w.wcsr_edges(), "wcsr")
+    g.plan(int(0.4 * g.ne * 8), block_bytes=64 << 10)
+    yield g
+    g.close()
+
+
+def want(O, g, algo, s):
+    return O.bfs(g, s) if algo == "bfs" else O.sssp(g, s)
+
+
+def test_serve_mixed_stream(T, O, g14w, eg):
+    src = O.sources(g14w, 48).tolist() + [1]
+    algos = ["sssp" if i % 5 == 0 else "bfs" for i in range(len(src))]
+    with T.Server(eg, max_slots=8, timeout_ms=20000) as sv:
+        tickets = [sv.submit(a, s) for a, s in zip(algos, src)]
+        for t, a, s in zip(tickets, algos, src):
+            vals, st = sv.wait(t)
+            w = want(O, g14w, a, s)
+            assert np.array_equal(vals, w), f"{a} {s}"
+            assert st["checksum"] == T.values_checksum(w)
+            assert st["status"] == 0 and st["latency_ms"] >= st["run_ms"]
+
+
+def test_serve_arrivals_join_running_traversal(T, O, g14w, eg):
+    src = O.sources(g14w, 24).tolist()
+    with T.Server(eg, max_slots=4, max_batch_iters=1, timeout_ms=20000) as sv:
+        tickets = []
+        for i, s in enumerate(src):
+            tickets.append((sv.submit("sssp" if i % 3 == 0 else "bfs", s), s, i))
+            time.sleep(0.0005 * (i % 4))
+        slots = set()
+        for t, s, i in tickets:
+            vals, st = sv.wait(t)
+            slots.add(st["slot"])
+            assert np.array_equal(vals, want(O, g14w, "sssp" if i % 3 == 0 else "bfs", s))
+        assert slots <= set(range(4))
+
+
+def test_serve_same_result_alone_and_in_mix(T, O, g14w, eg):
+    s0 = int(O.sources(g14w, 1)[0])
+    with T.Server(eg, max_slots=1) as sv:
+        alone, st_a = sv.wait(sv.submit("sssp", s0))
+    with T.Server(eg, max_slots=16) as sv:
+        ts = [sv.submit("bfs", s) for s in O.sources(g14w, 10)]
+        t0 = sv.submit("sssp", s0)
+        ts += [sv.submit("bfs", s) for s in O.sources(g14w, 20)[10:]]
+        mixed, st_m = sv.wait(t0)
+        for t in ts:
+            sv.wait(t)
+    assert np.array_equal(alone, mixed) and st_a["checksum"] == st_m["checksum"]
+
+
+def test_serve_memory_admission(T, O, g14w, eg):
+    per_slot = eg.nv * 4
+    with T.Server(eg, max_slots=64, mem_budget_bytes=3 * per_slot) as sv:
+        ts = [(sv.submit("bfs", s), s) for s in O.sources(g14w, 12)]
+        used = set()
+        for t, s in ts:
+            vals, st = sv.wait(t)
+            used.add(st["slot"])
+            assert np.array_equal(vals, O.bfs(g14w, s))
+        assert used <= {0, 1, 2}
+    with pytest.raises(T.ThvError) as e:
+        T.Server(eg, mem_budget_bytes=per_slot - 1)
+    assert e.value.status == T.THV_ENOMEM
+
+
+def test_serve_checksum_only_and_poll(T, O, g14w, eg):
+    with T.Server(eg) as sv:
+        t = sv.submit("bfs", int(O.sources(g14w, 1)[0]), want_values=False)
+        res = None
+        for _ in range(20000):
+            res = sv.poll(t)
+            if res is not None:
+                break
+            time.sleep(0.001)
+        vals, st = res
+        assert vals is None
+        assert st["checksum"] == T.values_checksum(O.bfs(g14w, int(O.sources(g14w, 1)[0])))
+
+
+def test_serve_rejects_bad_requests(T, O, g14w, eg):
+    with T.Server(eg) as sv:
+        with pytest.raises(T.ThvError):
+            sv.submit("bfs", eg.nv)
+        with pytest.raises(T.ThvError):
+            sv.submit("cc", 1)
+    gu = T.Graph.from_arrays(g14w.off, g14w.adj, "csr")
+    with T.Server(gu) as sv:
+        with pytest.raises(T.ThvError):
+            sv.submit("sssp", 1)
+    gu.close()

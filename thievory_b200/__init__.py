@@ -48,7 +48,8 @@ class _RunOpts(ctypes.Structure):
     _fields_ = [("source", ctypes.c_uint32), ("pr_iters", ctypes.c_uint32),
                 ("pr_damping", ctypes.c_double), ("sssp_delta", ctypes.c_uint32),
                 ("timeout_ms", ctypes.c_uint32), ("stream", ctypes.c_void_p),
-                ("small_degree", ctypes.c_uint32), ("chunk_edges", ctypes.c_uint32)]
+                ("small_degree", ctypes.c_uint32), ("chunk_edges", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
 
 
 class _Stats(ctypes.Structure):
@@ -56,7 +57,8 @@ class _Stats(ctypes.Structure):
                 ("iterations", ctypes.c_uint64), ("edges_expanded", ctypes.c_uint64),
                 ("hbm_edge_bytes", ctypes.c_uint64), ("link_edge_bytes", ctypes.c_uint64),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
-                ("kernel_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+                ("kernel_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+                ("checksum", ctypes.c_uint64)]
 
     def to_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
@@ -88,22 +90,24 @@ class _RmatOpts(ctypes.Structure):
 class _BatchOpts(ctypes.Structure):
     _fields_ = [("group", ctypes.c_uint32), ("timeout_ms", ctypes.c_uint32),
                 ("stream", ctypes.c_void_p), ("small_degree", ctypes.c_uint32),
-                ("chunk_edges", ctypes.c_uint32)]
+                ("chunk_edges", ctypes.c_uint32), ("sssp_delta", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32)]
 
 
 class _ServeOpts(ctypes.Structure):
     _fields_ = [("max_slots", ctypes.c_uint32), ("queue_capacity", ctypes.c_uint32),
                 ("mem_budget_bytes", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32),
-                ("pad", ctypes.c_uint32)]
+                ("max_batch_iters", ctypes.c_uint32)]
 
 
 class _QueryStats(ctypes.Structure):
-    _fields_ = [("submit_to_start_ms", ctypes.c_double), ("start_to_done_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double), ("iterations", ctypes.c_uint32),
-                ("slot", ctypes.c_uint32)]
+    _fields_ = [("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double), ("checksum", ctypes.c_uint64),
+                ("iterations", ctypes.c_uint32), ("slot", ctypes.c_uint32),
+                ("status", ctypes.c_int32), ("pad", ctypes.c_uint32)]
 
     def to_dict(self) -> dict:
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
 # Every function include/thv.h declares (tests check the library exports them).
@@ -112,7 +116,7 @@ ABI_FUNCTIONS = [
     "thv_info", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_run",
     "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
-    "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
+    "thv_pick_sources", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
     "thv_debug_fail_alloc_after",
 ]
 
@@ -142,15 +146,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_get_plan": ([P, ctypes.POINTER(_PlanInfo)], I32),
         "thv_get_blocks": ([P, U64, P, P, ctypes.POINTER(ctypes.c_uint64)], I32),
         "thv_link_bandwidth": ([I32, U64, ctypes.POINTER(D), ctypes.POINTER(D)], I32),
+        "thv_pick_sources": ([P, U64, U32, P], I32),
         "thv_run": ([P, U32, ctypes.POINTER(_RunOpts), P, ctypes.POINTER(_Stats)], I32),
         "thv_values": ([P, P], I32),
         "thv_write_values": ([ctypes.c_char_p, P, U64, U32], I32),
         "thv_batch_run": ([P, U32, P, U32, ctypes.POINTER(_BatchOpts), P, P,
                            ctypes.POINTER(_Stats)], I32),
         "thv_serve_start": ([P, ctypes.POINTER(_ServeOpts), pp], I32),
-        "thv_serve_submit": ([P, U32, U32, ctypes.POINTER(ctypes.c_uint64)], I32),
-        "thv_serve_poll": ([P, U64, P, ctypes.POINTER(_QueryStats)], I32),
-        "thv_serve_wait": ([P, U64, P, ctypes.POINTER(_QueryStats), U32], I32),
+        "thv_serve_submit": ([P, U32, U32, P, ctypes.POINTER(ctypes.c_uint64)], I32),
+        "thv_serve_poll": ([P, U64, ctypes.POINTER(_QueryStats)], I32),
+        "thv_serve_wait": ([P, U64, ctypes.POINTER(_QueryStats), U32], I32),
         "thv_serve_stop": ([P], I32),
         "thv_last_error": ([], ctypes.c_char_p),
         "thv_status_str": ([I32], ctypes.c_char_p),
@@ -255,11 +260,12 @@ class Graph:
     def run(self, algo: str, source: int = 1, pr_iters: int = 20, pr_damping: float = 0.85,
             out: Optional[np.ndarray] = None, want_values: bool = True, stream: int = 0,
             sssp_delta: int = 0, timeout_ms: int = 0, small_degree: int = 0,
-            chunk_edges: int = 0):
+            chunk_edges: int = 0, checksum: bool = False):
         """Run algo; returns (values or None, stats dict)."""
         lib = load_library()
         o = _RunOpts(source, pr_iters, pr_damping, sssp_delta, timeout_ms,
-                     ctypes.c_void_p(stream) if stream else None, small_degree, chunk_edges)
+                     ctypes.c_void_p(stream) if stream else None, small_degree, chunk_edges,
+                     1 if checksum else 0, 0)
         st = _Stats()
         buf = None
         if want_values:
@@ -275,19 +281,25 @@ class Graph:
 
     def batch_run(self, algo: str, sources: Sequence[int], group: int = 64,
                   want_values: bool = True, stream: int = 0, small_degree: int = 0,
-                  chunk_edges: int = 0, timeout_ms: int = 0):
+                  chunk_edges: int = 0, timeout_ms: int = 0, sssp_delta: int = 0):
         """Batched BFS/SSSP; returns (values [n, nv] or None, checksums [n], stats)."""
         lib = load_library()
         src = np.ascontiguousarray(sources, dtype=np.uint32)
         out = np.empty((len(src), self.nv), dtype=np.uint32) if want_values else None
         sums = np.empty(len(src), dtype=np.uint64)
         o = _BatchOpts(group, timeout_ms, ctypes.c_void_p(stream) if stream else None,
-                       small_degree, chunk_edges)
+                       small_degree, chunk_edges, sssp_delta, 0)
         st = _Stats()
         _check(lib.thv_batch_run(self._h, ALGO[algo], _ptr(src), len(src), ctypes.byref(o),
                                  None if out is None else _ptr(out), _ptr(sums),
                                  ctypes.byref(st)), f"thv_batch_run({algo})")
         return out, sums, st.to_dict()
+
+    def pick_sources(self, n: int, seed: int = 0x54484592) -> np.ndarray:
+        """n seeded sources uniform over vertices with out-degree > 0."""
+        out = np.empty(n, np.uint32)
+        _check(load_library().thv_pick_sources(self._h, seed, n, _ptr(out)), "thv_pick_sources")
+        return out
 
     def save(self, path: str) -> None:
         _check(load_library().thv_save(self._h, path.encode()), "thv_save")
@@ -327,44 +339,57 @@ class Graph:
 
 
 class Server:
-    """Continuous-batching query server over a Graph (thv_serve_*)."""
+    """Continuous-batching query server over a Graph (thv_serve_*).
+
+    submit() never blocks; results land in the array given at submit time
+    (kept alive here until the ticket completes)."""
 
     def __init__(self, graph: Graph, max_slots: int = 64, queue_capacity: int = 0,
-                 mem_budget_bytes: int = 0, timeout_ms: int = 0):
+                 mem_budget_bytes: int = 0, timeout_ms: int = 0, max_batch_iters: int = 0):
         lib = load_library()
         self.graph = graph
-        o = _ServeOpts(max_slots, queue_capacity, mem_budget_bytes, timeout_ms, 0)
+        self._bufs = {}
+        o = _ServeOpts(max_slots, queue_capacity, mem_budget_bytes, timeout_ms, max_batch_iters)
         self._h = ctypes.c_void_p()
         _check(lib.thv_serve_start(graph._h, ctypes.byref(o), ctypes.byref(self._h)),
                "thv_serve_start")
 
-    def submit(self, algo: str, source: int) -> int:
+    def submit(self, algo: str, source: int, want_values: bool = True) -> int:
+        out = np.empty(self.graph.nv, np.uint32) if want_values else None
         t = ctypes.c_uint64()
-        _check(load_library().thv_serve_submit(self._h, ALGO[algo], source, ctypes.byref(t)),
-               "thv_serve_submit")
+        _check(load_library().thv_serve_submit(self._h, ALGO[algo], int(source),
+                                               None if out is None else _ptr(out),
+                                               ctypes.byref(t)), "thv_serve_submit")
+        self._bufs[int(t.value)] = out
         return int(t.value)
 
-    def poll(self, ticket: int, want_values: bool = True):
-        out = np.empty(self.graph.nv, np.uint32) if want_values else None
+    def poll(self, ticket: int):
+        """None while running; else (values or None, stats dict)."""
         qs = _QueryStats()
-        s = load_library().thv_serve_poll(self._h, ticket, None if out is None else _ptr(out),
-                                          ctypes.byref(qs))
+        s = load_library().thv_serve_poll(self._h, ticket, ctypes.byref(qs))
         if s == THV_ENOTREADY:
             return None
+        out = self._bufs.pop(ticket, None)
         _check(s, "thv_serve_poll")
         return out, qs.to_dict()
 
-    def wait(self, ticket: int, timeout_ms: int = 60000, want_values: bool = True):
-        out = np.empty(self.graph.nv, np.uint32) if want_values else None
+    def wait(self, ticket: int, timeout_ms: int = 60000):
         qs = _QueryStats()
-        _check(load_library().thv_serve_wait(self._h, ticket, None if out is None else _ptr(out),
-                                             ctypes.byref(qs), timeout_ms), "thv_serve_wait")
+        s = load_library().thv_serve_wait(self._h, ticket, ctypes.byref(qs), timeout_ms)
+        out = self._bufs.pop(ticket, None)
+        _check(s, "thv_serve_wait")
         return out, qs.to_dict()
 
     def stop(self) -> None:
         if self._h:
-            _check(load_library().thv_serve_stop(self._h), "thv_serve_stop")
-            self._h = None
+            h, self._h = self._h, None
+            _check(load_library().thv_serve_stop(h), "thv_serve_stop")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
 
 
 # ---------------------------------------------------------------------------

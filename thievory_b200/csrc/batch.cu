@@ -640,7 +640,7 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
   a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0x7FFFFFF0ull) * 2 + 8;
   a.small_deg = small;
   a.chunk = chunk;
-  a.delta = 2;
+  a.delta = o && o->sssp_delta ? o->sssp_delta : 2u;
   thv_stats local{};
   uint32_t launches = 0;
   float dev_ms = 0.f;

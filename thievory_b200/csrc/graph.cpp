@@ -681,6 +681,31 @@ thv_status thv_batch_run(thv_graph *g, thv_algo algo, const uint32_t *sources,
   THV_GUARD_END
 }
 
+static uint64_t mix64_host(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+thv_status thv_pick_sources(const thv_graph *g, uint64_t seed, uint32_t n, uint32_t *out) {
+  if (!g || (!out && n)) return fail(THV_EINVAL, "null argument");
+  if (g->nv == 0) return fail(THV_EINVAL, "empty graph");
+  const uint64_t key = mix64_host(seed ^ 0x534F555243455331ull);
+  for (uint32_t j = 0; j < n; j++) {
+    bool found = false;
+    for (uint64_t t = 0; t < (1ull << 24) && !found; t++) {
+      const uint64_t c = mix64_host(key ^ (((uint64_t)j << 24) | t)) % g->nv;
+      if (g->off[c + 1] > g->off[c]) {
+        out[j] = (uint32_t)c;
+        found = true;
+      }
+    }
+    if (!found) return fail(THV_EINVAL, "no vertex with out-degree > 0");
+  }
+  return THV_OK;
+}
+
 const char *thv_last_error(void) { return g_last_error.c_str(); }
 
 const char *thv_status_str(thv_status s) {

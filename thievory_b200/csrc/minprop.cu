@@ -56,6 +56,7 @@ struct MinCtrl {
   unsigned long long cnt_small[3], cnt_big[3], remaining[3], wc[3];
   unsigned minkept[3], pad;
   unsigned long long edges, hbm_bytes, link_bytes, vertices;
+  unsigned long long checksum;
 };
 
 struct MinArgs {
@@ -419,6 +420,28 @@ __global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
   }
 }
 
+__global__ void values_checksum_kernel(const uint32_t *val, uint64_t nv,
+                                       unsigned long long *sum) {
+  __shared__ unsigned long long s_red[32];
+  unsigned long long h = 0;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    unsigned long long x = (v << 32) | val[v];
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    h += x ^ (x >> 31);
+  }
+  h = warp_sum(h);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = h;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    h = threadIdx.x < (blockDim.x >> 5) ? s_red[threadIdx.x] : 0ull;
+    h = warp_sum(h);
+    if (threadIdx.x == 0) atomicAdd(sum, h);
+  }
+}
+
 // ------------------------------------------------------------------ host --
 
 static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
@@ -549,6 +572,13 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   }
   if (s != THV_OK) return s;
   THV_CUDA(cudaEventRecord(ms->ev1, st));
+  const bool want_sum = o && (o->flags & THV_RUN_CHECKSUM);
+  if (want_sum) {
+    const int cgrid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 255) / 256)));
+    values_checksum_kernel<<<cgrid, 256, 0, st>>>(ms->d_val, g->nv, &ms->d_ctrl->checksum);
+    THV_CUDA(cudaGetLastError());
+    launches++;
+  }
   THV_CUDA(cudaMemcpyAsync(ms->h_ctrl, ms->d_ctrl, sizeof(MinCtrl),
                            cudaMemcpyDeviceToHost, st));
   THV_CUDA(cudaStreamSynchronize(st));
@@ -564,6 +594,7 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
     stats->link_edge_bytes = hc.link_bytes;
     stats->kernel_launches = launches;
     stats->d2h_bytes += sizeof(MinCtrl);
+    stats->checksum = want_sum ? hc.checksum : 0;
   }
   if (hc.err == kDevErrBarrier)
     return fail(THV_ETIMEOUT, "grid barrier wait exceeded %u ms", tmo);

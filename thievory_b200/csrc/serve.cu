@@ -1,0 +1,754 @@
+// Serving: continuous batching of BFS / SSSP queries over one resident graph.
+//
+// No counterpart in the reference (one query per process, src/main.cu:152).
+// Up to 64 queries occupy the slots of a single traversal state
+//   val[v][slot]   u32, value + 1 in the single-source encoding (n+1 unset)
+//   front[v]       u64 mask of slots for which v is pending
+// driven by the frontier machinery of the single-source engine (pending
+// bitmap, ballot compaction into small-vertex groups and high-degree chunks,
+// zero-copy addressing), with per-slot near/far thresholds so that queries
+// admitted at different times coexist.  BFS slots relax with unit weights
+// (distance + 1 == level + 1, window 1: exactly level-synchronous); SSSP
+// slots use the edge weights with window 2.
+//
+// The persistent kernel returns to the host when any slot's query has no
+// pending vertex left, or after a bounded number of iterations when
+// requests are waiting.  The host dispatcher thread then writes finished
+// slots' results (one column of val) into the caller's buffers, resets the
+// column, admits waiting requests into free slots (seeding their sources)
+// and relaunches: a request that arrives while others run joins at the next
+// launch boundary and shares every later edge read with them.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "thv_device.cuh"
+#include "thv_internal.h"
+
+namespace thv {
+
+constexpr int kSvThreads = 512;
+constexpr uint32_t kSvMaxSlots = 64;
+constexpr uint32_t kSvDeltaSssp = 2;
+
+struct SvCtrl {
+  GridBar bar;
+  unsigned err, iters;
+  unsigned long long cnt_small[3], cnt_big[3], wc[3];
+  unsigned long long taken_or[3], alive_or[3];
+  unsigned thr[kSvMaxSlots], step[kSvMaxSlots];
+  unsigned long long done_mask;
+  unsigned long long edges, hbm_bytes, link_bytes, pairs;
+};
+
+struct SvArgs {
+  const uint64_t *off;
+  const uint32_t *blk_vb;
+  const uint64_t *blk_base;
+  uint64_t host_base;
+  uint32_t *val;  // [nv][W]
+  unsigned long long *front;
+  uint32_t *bm;
+  WorkItem *qs, *qb;
+  unsigned long long *qsm, *qbm;
+  unsigned long long cap_s, cap_b;
+  SvCtrl *ctrl;
+  unsigned long long active, unit;
+  unsigned long long timeout_ns;
+  uint32_t nblk, nv, ngroups, W;
+  uint32_t max_iters, small_deg, chunk, pad;
+};
+
+__device__ __forceinline__ unsigned long long warp_or(unsigned long long x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x |= __shfl_xor_sync(kFull, x, d);
+  return x;
+}
+
+__device__ __forceinline__ void sv_edge(const SvArgs &a, uint32_t u, uint32_t w, uint32_t wt,
+                                        unsigned long long f) {
+  const uint32_t *du = a.val + (size_t)u * a.W;
+  uint32_t *dw = a.val + (size_t)w * a.W;
+  unsigned long long improved = 0;
+  while (f) {
+    const int s = __ffsll((long long)f) - 1;
+    f &= f - 1;
+    const unsigned long long cand =
+        (unsigned long long)ldcg(du + s) + (((a.unit >> s) & 1ull) ? 1u : wt);
+    if (cand < ldcg(dw + s)) {
+      const uint32_t old = atomicMin(dw + s, (uint32_t)cand);
+      if (cand < old) improved |= 1ull << s;
+    }
+  }
+  if (improved) {
+    atomicOr(a.front + w, improved);
+    const uint32_t m = 1u << (w & 31u);
+    uint32_t *bp = a.bm + (w >> 5);
+    if (!(ldcg(bp) & m)) atomicOr(bp, m);
+  }
+}
+
+template <int ESZ>
+__device__ __forceinline__ void sv_chunk(const SvArgs &a, const WorkItem &it, unsigned long long f) {
+  constexpr int PER = 16 / ESZ;
+  const unsigned lane = lane_id();
+  const uintptr_t start = it.eaddr;
+  const uintptr_t end = start + (uintptr_t)it.cnt * ESZ;
+  for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end; p += 512u) {
+    const uint4 q = ld_nc_v4(p);
+    const uint32_t e[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const uintptr_t ea = p + (uintptr_t)ESZ * j;
+      if (ea >= start && ea < end)
+        sv_edge(a, it.v, ESZ == 4 ? e[j] : e[2 * j], ESZ == 4 ? 1u : e[2 * j + 1], f);
+    }
+  }
+}
+
+template <int ESZ>
+__device__ __forceinline__ void sv_group(const SvArgs &a, unsigned long long first,
+                                         unsigned long long n_small) {
+  const unsigned lane = lane_id();
+  const unsigned long long idx = first + lane;
+  WorkItem it{0, 0, 0};
+  unsigned long long f = 0;
+  if (idx < n_small) {
+    it = a.qs[idx];
+    f = a.qsm[idx];
+  }
+  const unsigned incl = warp_incl_scan<unsigned>(it.cnt);
+  const unsigned excl = incl - it.cnt;
+  const unsigned total = __shfl_sync(kFull, incl, 31);
+  for (unsigned k = 0; k < total; k += 32) {
+    const unsigned t = k + lane;
+    const int o = warp_owner(excl, t);
+    const unsigned long long ea = shfl64(it.eaddr, o);
+    const unsigned oex = __shfl_sync(kFull, excl, o);
+    const unsigned ou = __shfl_sync(kFull, it.v, o);
+    const unsigned long long of = shfl64(f, o);
+    if (t < total) {
+      const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
+      if (ESZ == 4) {
+        sv_edge(a, ou, ld_nc_u32(addr), 1u, of);
+      } else {
+        const uint2 e = ld_nc_u2(addr);
+        sv_edge(a, ou, e.x, e.y, of);
+      }
+    }
+  }
+}
+
+template <int ESZ>
+__global__ void __launch_bounds__(kSvThreads) sv_kernel(SvArgs a) {
+  extern __shared__ uint32_t s_dyn[];
+  __shared__ uint32_t s_thr[kSvMaxSlots], s_step[kSvMaxSlots];
+  uint32_t *s_vb = s_dyn;
+  const bool smem_tab = a.nblk <= kSmemBlocks;
+  if (smem_tab)
+    for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x) s_vb[i] = a.blk_vb[i];
+  for (uint32_t s = threadIdx.x; s < kSvMaxSlots; s += blockDim.x) {
+    s_thr[s] = ldcg(&a.ctrl->thr[s]);
+    s_step[s] = ldcg(&a.ctrl->step[s]);
+  }
+  __syncthreads();
+  const uint32_t *vb = smem_tab ? s_vb : a.blk_vb;
+  SvCtrl *c = a.ctrl;
+  const unsigned lane = lane_id();
+  const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  unsigned iter = 0;
+  unsigned long long done = 0;
+  for (; iter < a.max_iters; ++iter) {
+    const unsigned slot = iter % 3, nslot = (iter + 1) % 3;
+    if (leader) {
+      c->cnt_small[nslot] = 0;
+      c->cnt_big[nslot] = 0;
+      c->wc[nslot] = 0;
+      c->taken_or[nslot] = 0;
+      c->alive_or[nslot] = 0;
+    }
+    // ---------------------------------------------------------- compaction
+    unsigned long long my_taken = 0, my_alive = 0, my_edges = 0, my_hbm = 0, my_link = 0,
+                       my_pairs = 0;
+    for (unsigned g = gwarp; g < a.ngroups; g += nwarps) {
+      const unsigned wbase = g * 32u;
+      const uint32_t word = ldcg(a.bm + wbase + lane);
+      unsigned nz = __ballot_sync(kFull, word != 0);
+      while (nz) {
+        const int j = __ffs(nz) - 1;
+        nz &= nz - 1;
+        const uint32_t wd = __shfl_sync(kFull, word, j);
+        const uint32_t v = (wbase + j) * 32u + lane;
+        unsigned long long take = 0, keep = 0;
+        if ((wd >> lane) & 1u) {
+          const unsigned long long f = ldcg(a.front + v);
+          const uint32_t *dv = a.val + (size_t)v * a.W;
+          unsigned long long r = f;
+          while (r) {
+            const int s = __ffsll((long long)r) - 1;
+            r &= r - 1;
+            if (ldcg(dv + s) < s_thr[s]) take |= 1ull << s;
+          }
+          keep = f & ~take;
+          a.front[v] = keep;
+          my_alive |= f;
+          my_taken |= take;
+        }
+        const unsigned km = __ballot_sync(kFull, keep != 0);
+        if (lane == 0) a.bm[wbase + j] = km;
+        uint32_t deg = 0;
+        unsigned long long eaddr = 0;
+        if (take) {
+          const uint64_t s0 = __ldg(a.off + v), e0 = __ldg(a.off + v + 1);
+          deg = (uint32_t)(e0 - s0);
+          const unsigned long long base = __ldg(a.blk_base + find_block(vb, a.nblk, v));
+          eaddr = base + s0 * ESZ;
+          my_edges += deg;
+          my_pairs += __popcll(take);
+          if (base == a.host_base) my_link += (unsigned long long)deg * ESZ;
+          else my_hbm += (unsigned long long)deg * ESZ;
+        }
+        const bool small = take && deg > 0 && deg < a.small_deg;
+        const bool big = take && deg >= a.small_deg;
+        const unsigned sm = __ballot_sync(kFull, small);
+        if (sm) {
+          const int ldr = __ffs(sm) - 1;
+          unsigned long long base = 0;
+          if (lane == (unsigned)ldr)
+            base = atomicAdd(&c->cnt_small[slot], (unsigned long long)__popc(sm));
+          base = shfl64(base, ldr);
+          const unsigned long long pos = base + __popc(sm & lanemask_lt());
+          if (small) {
+            if (pos < a.cap_s) {
+              a.qs[pos] = WorkItem{eaddr, v, deg};
+              a.qsm[pos] = take;
+            } else {
+              atomicCAS(&c->err, 0u, kDevErrQueue);
+            }
+          }
+        }
+        if (__any_sync(kFull, big)) {
+          const unsigned nch = big ? (deg + a.chunk - 1) / a.chunk : 0u;
+          const unsigned inc = warp_incl_scan<unsigned>(nch);
+          const unsigned tot = __shfl_sync(kFull, inc, 31);
+          unsigned long long base = 0;
+          if (lane == 0) base = atomicAdd(&c->cnt_big[slot], (unsigned long long)tot);
+          base = shfl64(base, 0);
+          if (big) {
+            unsigned long long pos = base + inc - nch;
+            for (unsigned k = 0; k < nch; k++, pos++) {
+              const uint32_t lo = k * a.chunk;
+              if (pos < a.cap_b) {
+                a.qb[pos] = WorkItem{eaddr + (unsigned long long)lo * ESZ, v, min(a.chunk, deg - lo)};
+                a.qbm[pos] = take;
+              } else {
+                atomicCAS(&c->err, 0u, kDevErrQueue);
+              }
+            }
+          }
+        }
+      }
+    }
+    my_taken = warp_or(my_taken);
+    my_alive = warp_or(my_alive);
+    my_edges = warp_sum(my_edges);
+    my_hbm = warp_sum(my_hbm);
+    my_link = warp_sum(my_link);
+    my_pairs = warp_sum(my_pairs);
+    if (lane == 0) {
+      if (my_taken) atomicOr(&c->taken_or[slot], my_taken);
+      if (my_alive) atomicOr(&c->alive_or[slot], my_alive);
+      if (my_pairs) {
+        atomicAdd(&c->edges, my_edges);
+        atomicAdd(&c->hbm_bytes, my_hbm);
+        atomicAdd(&c->link_bytes, my_link);
+        atomicAdd(&c->pairs, my_pairs);
+      }
+    }
+    if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+    const unsigned long long taken = ldcg(&c->taken_or[slot]);
+    const unsigned long long alive = ldcg(&c->alive_or[slot]);
+    done = a.active & ~alive;
+    const unsigned long long ns = ldcg(&c->cnt_small[slot]);
+    const unsigned long long nb = ldcg(&c->cnt_big[slot]);
+    // ----------------------------------------------------------- expansion
+    const unsigned long long ntask = nb + (ns + 31) / 32;
+    for (unsigned long long t = gwarp; t < ntask;) {
+      if (t < nb) sv_chunk<ESZ>(a, a.qb[t], a.qbm[t]);
+      else sv_group<ESZ>(a, (t - nb) * 32ull, ns);
+      unsigned long long nt = 0;
+      if (lane == 0) nt = nwarps + atomicAdd(&c->wc[slot], 1ull);
+      t = shfl64(nt, 0);
+    }
+    // per-slot windows (one thread per slot; every block computes the same
+    // values from the same masks): a slot that expanded something moves by
+    // its base width, a pending slot with nothing in its window doubles its
+    // step, so a gap in its distances closes in a few iterations
+    if (threadIdx.x < kSvMaxSlots && ((a.active >> threadIdx.x) & 1ull)) {
+      const uint32_t s = threadIdx.x;
+      const uint32_t base = ((a.unit >> s) & 1ull) ? 1u : kSvDeltaSssp;
+      uint32_t st = s_step[s];
+      if ((taken >> s) & 1ull) st = base;
+      else if ((alive >> s) & 1ull) st = min(st * 2u, 1u << 30);
+      s_step[s] = st;
+      s_thr[s] = (uint32_t)min((unsigned long long)s_thr[s] + st, 0xFFFFFFFFull);
+    }
+    if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+    if (done) {
+      ++iter;
+      break;
+    }
+  }
+  if (leader) {
+    c->iters = iter;
+    c->done_mask = done;
+    for (uint32_t s = 0; s < kSvMaxSlots; s++) {
+      c->thr[s] = s_thr[s];
+      c->step[s] = s_step[s];
+    }
+  }
+}
+
+__global__ void sv_reset(SvArgs a, uint32_t nw_alloc) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t inf = a.nv + 1u;
+  for (uint64_t i = tid; i < (uint64_t)a.nv * a.W; i += stride) a.val[i] = inf;
+  for (uint64_t v = tid; v < a.nv; v += stride) a.front[v] = 0;
+  for (uint64_t w = tid; w < nw_alloc; w += stride) a.bm[w] = 0;
+  if (tid == 0) memset(a.ctrl, 0, sizeof(SvCtrl));
+}
+
+struct SvSeed {
+  uint32_t slot, source, thr, step;
+};
+
+__global__ void sv_seed(SvArgs a, const SvSeed *seeds, uint32_t n) {
+  const uint32_t i = threadIdx.x;
+  if (i >= n) return;
+  const SvSeed sd = seeds[i];
+  a.val[(size_t)sd.source * a.W + sd.slot] = 1;
+  atomicOr(a.front + sd.source, 1ull << sd.slot);
+  atomicOr(a.bm + (sd.source >> 5), 1u << (sd.source & 31u));
+  a.ctrl->thr[sd.slot] = sd.thr;
+  a.ctrl->step[sd.slot] = sd.step;
+}
+
+__device__ __forceinline__ unsigned long long sv_hash(uint32_t v, uint32_t val) {
+  unsigned long long x = ((unsigned long long)v << 32) | val;
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Column `slot` -> out (may be null), checksum, and reset for reuse.
+__global__ void sv_extract(SvArgs a, uint32_t slot, uint32_t *out, unsigned long long *sum) {
+  __shared__ unsigned long long s_red[32];
+  const uint32_t inf = a.nv + 1u;
+  unsigned long long h = 0;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < a.nv;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t *p = a.val + v * a.W + slot;
+    const uint32_t x = *p;
+    *p = inf;
+    if (out) out[v] = x;
+    h += sv_hash((uint32_t)v, x);
+  }
+  h = warp_sum(h);
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = h;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    h = threadIdx.x < (blockDim.x >> 5) ? s_red[threadIdx.x] : 0ull;
+    h = warp_sum(h);
+    if (threadIdx.x == 0) atomicAdd(sum, h);
+  }
+}
+
+}  // namespace thv
+
+// ================================================================== server
+
+using namespace thv;
+
+namespace {
+
+struct Query {
+  thv_algo algo;
+  uint32_t source;
+  uint32_t *out;
+  double t_submit = 0, t_start = 0, t_done = 0;
+  uint32_t slot = 0, iter_start = 0, iterations = 0;
+  uint64_t checksum = 0;
+  thv_status status = THV_OK;
+  bool done = false;
+};
+
+}  // namespace
+
+struct thv_server {
+  thv_graph *g = nullptr;
+  uint32_t W = 0, queue_cap = 0, batch_iters = 4;
+  uint64_t timeout_ns = 0;
+  // device state
+  uint32_t *d_val = nullptr, *d_bm = nullptr, *d_out = nullptr;
+  unsigned long long *d_front = nullptr, *d_qsm = nullptr, *d_qbm = nullptr, *d_sum = nullptr;
+  WorkItem *d_qs = nullptr, *d_qb = nullptr;
+  uint64_t cap_s = 0, cap_b = 0;
+  SvCtrl *d_ctrl = nullptr, *h_ctrl = nullptr;
+  SvSeed *d_seeds = nullptr, *h_seeds = nullptr;
+  unsigned long long *h_sum = nullptr;
+  uint32_t ngroups = 0;
+  cudaStream_t st = nullptr;
+  // host state
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<uint64_t> waiting;
+  std::map<uint64_t, Query> queries;
+  uint64_t next_ticket = 1;
+  uint64_t slot_ticket[kSvMaxSlots] = {};
+  unsigned long long active = 0, unit = 0;
+  uint64_t total_iters = 0;
+  bool stopping = false;
+  thv_status fatal = THV_OK;
+  std::string fatal_msg;
+  std::thread worker;
+};
+
+namespace {
+
+double clock_ms() {
+  return std::chrono::duration<double, std::milli>(
+             std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void server_free(thv_server *s) {
+  dev_free(s->d_val);
+  dev_free(s->d_bm);
+  dev_free(s->d_out);
+  dev_free(s->d_front);
+  dev_free(s->d_qsm);
+  dev_free(s->d_qbm);
+  dev_free(s->d_sum);
+  dev_free(s->d_qs);
+  dev_free(s->d_qb);
+  dev_free(s->d_ctrl);
+  pinned_free(s->h_ctrl);
+  dev_free(s->d_seeds);
+  pinned_free(s->h_seeds);
+  pinned_free(s->h_sum);
+  if (s->st) cudaStreamDestroy(s->st);
+}
+
+SvArgs make_args(thv_server *s) {
+  thv_graph *g = s->g;
+  SvArgs a{};
+  a.off = g->d_off;
+  a.blk_vb = g->plan.d_vbegin;
+  a.blk_base = g->plan.d_base;
+  a.host_base = g->h_edges_dev;
+  a.val = s->d_val;
+  a.front = s->d_front;
+  a.bm = s->d_bm;
+  a.qs = s->d_qs;
+  a.qb = s->d_qb;
+  a.qsm = s->d_qsm;
+  a.qbm = s->d_qbm;
+  a.cap_s = s->cap_s;
+  a.cap_b = s->cap_b;
+  a.ctrl = s->d_ctrl;
+  a.timeout_ns = s->timeout_ns;
+  a.nblk = (uint32_t)g->plan.blocks.size();
+  a.nv = (uint32_t)g->nv;
+  a.ngroups = s->ngroups;
+  a.W = s->W;
+  a.small_deg = 64;
+  a.chunk = 256;
+  return a;
+}
+
+// One launch of the serving kernel; returns the finished-slot mask.
+thv_status step(thv_server *s, uint32_t max_iters, unsigned long long *done, uint32_t *iters) {
+  thv_graph *g = s->g;
+  SvArgs a = make_args(s);
+  a.active = s->active;
+  a.unit = s->unit;
+  a.max_iters = max_iters;
+  const size_t smem = g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0;
+  void *kern = g->esz == 8 ? (void *)sv_kernel<8> : (void *)sv_kernel<4>;
+  int bpsm = 0;
+  if (g->esz == 8)
+    THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, sv_kernel<8>, kSvThreads, smem));
+  else
+    THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, sv_kernel<4>, kSvThreads, smem));
+  if (bpsm < 1) return fail(THV_ECUDA, "serving kernel cannot be resident");
+  void *args[] = {&a};
+  THV_CUDA(cudaLaunchCooperativeKernel(kern, dim3(bpsm * g->num_sms), dim3(kSvThreads), args, smem, s->st));
+  THV_CUDA(cudaMemcpyAsync(s->h_ctrl, s->d_ctrl, sizeof(SvCtrl), cudaMemcpyDeviceToHost, s->st));
+  THV_CUDA(cudaStreamSynchronize(s->st));
+  const SvCtrl &hc = *s->h_ctrl;
+  if (hc.err == kDevErrBarrier) return fail(THV_ETIMEOUT, "serving: grid barrier timeout");
+  if (hc.err) return fail(THV_EDEVICE, "serving: device error %u", hc.err);
+  *done = hc.done_mask;
+  *iters = hc.iters;
+  return THV_OK;
+}
+
+thv_status retire(thv_server *s, unsigned long long done) {
+  thv_graph *g = s->g;
+  SvArgs a = make_args(s);
+  const int grid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 255) / 256)));
+  while (done) {
+    const int slot = __builtin_ctzll(done);
+    done &= done - 1;
+    uint64_t ticket;
+    uint32_t *out;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      ticket = s->slot_ticket[slot];
+      out = s->queries[ticket].out;
+    }
+    THV_CUDA(cudaMemsetAsync(s->d_sum, 0, 8, s->st));
+    sv_extract<<<grid, 256, 0, s->st>>>(a, (uint32_t)slot, out ? s->d_out : nullptr, s->d_sum);
+    THV_CUDA(cudaGetLastError());
+    THV_CUDA(cudaMemcpyAsync(s->h_sum, s->d_sum, 8, cudaMemcpyDeviceToHost, s->st));
+    if (out) THV_CUDA(cudaMemcpyAsync(out, s->d_out, g->nv * 4, cudaMemcpyDeviceToHost, s->st));
+    THV_CUDA(cudaStreamSynchronize(s->st));
+    std::lock_guard<std::mutex> lk(s->mu);
+    Query &q = s->queries[ticket];
+    q.checksum = *s->h_sum;
+    q.t_done = clock_ms();
+    q.iterations = (uint32_t)(s->total_iters - q.iter_start);
+    q.done = true;
+    s->active &= ~(1ull << slot);
+    s->unit &= ~(1ull << slot);
+    s->slot_ticket[slot] = 0;
+  }
+  s->cv_done.notify_all();
+  return THV_OK;
+}
+
+void fail_all(thv_server *s, thv_status st, const std::string &msg) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->fatal = st;
+  s->fatal_msg = msg;
+  for (auto &kv : s->queries) {
+    if (!kv.second.done) {
+      kv.second.done = true;
+      kv.second.status = st;
+      kv.second.t_done = clock_ms();
+    }
+  }
+  s->waiting.clear();
+  s->active = 0;
+  s->cv_done.notify_all();
+}
+
+void worker_loop(thv_server *s) {
+  cudaSetDevice(s->g->device);
+  for (;;) {
+    uint32_t nseed = 0;
+    bool requests_waiting = false;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return s->stopping || !s->waiting.empty() || s->active; });
+      if (s->stopping && s->waiting.empty() && !s->active) return;
+      // admission: free slot (its column is reset) for each waiting query
+      while (!s->waiting.empty()) {
+        int slot = -1;
+        for (uint32_t i = 0; i < s->W; i++)
+          if (!((s->active >> i) & 1ull)) { slot = (int)i; break; }
+        if (slot < 0) break;
+        const uint64_t t = s->waiting.front();
+        s->waiting.pop_front();
+        Query &q = s->queries[t];
+        q.slot = (uint32_t)slot;
+        q.t_start = clock_ms();
+        q.iter_start = (uint32_t)s->total_iters;
+        const bool bfs = q.algo == THV_ALGO_BFS;
+        s->h_seeds[nseed++] = SvSeed{(uint32_t)slot, q.source, bfs ? 2u : 1u + kSvDeltaSssp,
+                                     bfs ? 1u : kSvDeltaSssp};
+        s->active |= 1ull << slot;
+        if (bfs) s->unit |= 1ull << slot;
+        s->slot_ticket[slot] = t;
+      }
+      // with a free slot, return to the host every few iterations so that a
+      // request arriving meanwhile is admitted quickly; with none free, run
+      // until a query finishes
+      requests_waiting = __builtin_popcountll(s->active) < (int)s->W;
+    }
+    if (nseed) {
+      SvArgs a = make_args(s);
+      if (cudaMemcpyAsync(s->d_seeds, s->h_seeds, nseed * sizeof(SvSeed), cudaMemcpyHostToDevice,
+                          s->st) != cudaSuccess) {
+        fail_all(s, THV_ECUDA, "seed copy failed");
+        return;
+      }
+      sv_seed<<<1, kSvMaxSlots, 0, s->st>>>(a, s->d_seeds, nseed);
+    }
+    unsigned long long done = 0;
+    uint32_t iters = 0;
+    const uint32_t budget = requests_waiting ? s->batch_iters : 1u << 20;
+    thv_status st = step(s, budget, &done, &iters);
+    if (st != THV_OK) {
+      fail_all(s, st, thv_last_error());
+      return;
+    }
+    s->total_iters += iters;
+    if (done && (st = retire(s, done)) != THV_OK) {
+      fail_all(s, st, thv_last_error());
+      return;
+    }
+  }
+}
+
+thv_status start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
+  if (g->fmt == THV_FMT_CSC) return fail(THV_EINVAL, "serving needs out-edges (CSR/WCSR)");
+  if (g->nv >= 0xFFFFFFFFull) return fail(THV_EUNSUPPORTED, "too many vertices");
+  THV_TRY(ensure_plan(g));
+  std::unique_ptr<thv_server, void (*)(thv_server *)> s(new thv_server(), [](thv_server *p) {
+    server_free(p);
+    delete p;
+  });
+  s->g = g;
+  uint32_t W = o && o->max_slots ? std::min<uint32_t>(o->max_slots, kSvMaxSlots) : kSvMaxSlots;
+  if (o && o->mem_budget_bytes) {
+    const uint64_t per_slot = g->nv * 4ull;
+    W = (uint32_t)std::min<uint64_t>(W, o->mem_budget_bytes / per_slot);
+    if (W == 0) return fail(THV_ENOMEM, "memory budget %llu below one slot (%llu bytes)",
+                            (unsigned long long)o->mem_budget_bytes, (unsigned long long)per_slot);
+  }
+  s->W = W;
+  s->queue_cap = o && o->queue_capacity ? o->queue_capacity : 65536u;
+  s->batch_iters = o && o->max_batch_iters ? o->max_batch_iters : 4u;
+  s->timeout_ns = (uint64_t)(o && o->timeout_ms ? o->timeout_ms : 60000u) * 1000000ull;
+  const uint64_t nw = (g->nv + 31) / 32;
+  s->ngroups = (uint32_t)((nw + 31) / 32);
+  const uint64_t nw_alloc = (uint64_t)s->ngroups * 32;
+  s->cap_s = g->nv + 32;
+  s->cap_b = g->ne / 256 + g->ne / 64 + 64;
+  THV_TRY(dev_alloc((void **)&s->d_val, g->nv * (uint64_t)W * 4 + 64, "serving values"));
+  THV_TRY(dev_alloc((void **)&s->d_front, g->nv * 8 + 64, "serving masks"));
+  THV_TRY(dev_alloc((void **)&s->d_bm, nw_alloc * 4, "serving bitmap"));
+  THV_TRY(dev_alloc((void **)&s->d_out, g->nv * 4 + 64, "serving output"));
+  THV_TRY(dev_alloc((void **)&s->d_qs, s->cap_s * sizeof(WorkItem), "serving queue"));
+  THV_TRY(dev_alloc((void **)&s->d_qsm, s->cap_s * 8, "serving queue masks"));
+  THV_TRY(dev_alloc((void **)&s->d_qb, s->cap_b * sizeof(WorkItem), "serving chunk queue"));
+  THV_TRY(dev_alloc((void **)&s->d_qbm, s->cap_b * 8, "serving chunk masks"));
+  THV_TRY(dev_alloc((void **)&s->d_ctrl, sizeof(SvCtrl), "serving control"));
+  THV_TRY(pinned_alloc((void **)&s->h_ctrl, sizeof(SvCtrl), "serving control"));
+  THV_TRY(dev_alloc((void **)&s->d_seeds, kSvMaxSlots * sizeof(SvSeed), "serving seeds"));
+  THV_TRY(pinned_alloc((void **)&s->h_seeds, kSvMaxSlots * sizeof(SvSeed), "serving seeds"));
+  THV_TRY(dev_alloc((void **)&s->d_sum, 8, "serving checksum"));
+  THV_TRY(pinned_alloc((void **)&s->h_sum, 8, "serving checksum"));
+  THV_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  SvArgs a = make_args(s.get());
+  const int grid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 255) / 256)));
+  sv_reset<<<grid, 256, 0, s->st>>>(a, (uint32_t)nw_alloc);
+  THV_CUDA(cudaGetLastError());
+  THV_CUDA(cudaStreamSynchronize(s->st));
+  thv_server *raw = s.release();
+  raw->worker = std::thread(worker_loop, raw);
+  *out = raw;
+  return THV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+thv_status thv_serve_start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
+  try {
+    if (!g || !out) return fail(THV_EINVAL, "null argument");
+    THV_CUDA(cudaSetDevice(g->device));
+    return start(g, o, out);
+  } catch (...) {
+    return fail(THV_ENOMEM, "serving start: host allocation failed");
+  }
+}
+
+thv_status thv_serve_submit(thv_server *s, thv_algo algo, uint32_t source, uint32_t *out,
+                            uint64_t *ticket) {
+  if (!s || !ticket) return fail(THV_EINVAL, "null argument");
+  if (algo != THV_ALGO_BFS && algo != THV_ALGO_SSSP)
+    return fail(THV_EINVAL, "serving runs BFS and SSSP queries");
+  if (algo == THV_ALGO_SSSP && !s->g->weighted) return fail(THV_EINVAL, "SSSP needs edge weights");
+  if (source >= s->g->nv) return fail(THV_EINVAL, "source %u out of range", source);
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->fatal != THV_OK) return fail(s->fatal, "server failed: %s", s->fatal_msg.c_str());
+  if (s->stopping) return fail(THV_EINVAL, "server is stopping");
+  if (s->waiting.size() >= s->queue_cap) return fail(THV_EBUSY, "serving queue full");
+  const uint64_t t = s->next_ticket++;
+  Query q;
+  q.algo = algo;
+  q.source = source;
+  q.out = out;
+  q.t_submit = clock_ms();
+  s->queries.emplace(t, q);
+  s->waiting.push_back(t);
+  *ticket = t;
+  s->cv_work.notify_one();
+  return THV_OK;
+}
+
+static thv_status collect(thv_server *s, uint64_t ticket, thv_query_stats *st) {
+  auto it = s->queries.find(ticket);
+  if (it == s->queries.end()) return fail(THV_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
+  if (!it->second.done) return THV_ENOTREADY;
+  const Query &q = it->second;
+  if (st) {
+    st->queue_ms = q.t_start > 0 ? q.t_start - q.t_submit : 0;
+    st->run_ms = q.t_start > 0 ? q.t_done - q.t_start : 0;
+    st->latency_ms = q.t_done - q.t_submit;
+    st->checksum = q.checksum;
+    st->iterations = q.iterations;
+    st->slot = q.slot;
+    st->status = q.status;
+  }
+  const thv_status qs = q.status;
+  s->queries.erase(it);
+  return qs == THV_OK ? THV_OK : fail(qs, "query failed");
+}
+
+thv_status thv_serve_poll(thv_server *s, uint64_t ticket, thv_query_stats *st) {
+  if (!s) return fail(THV_EINVAL, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  return collect(s, ticket, st);
+}
+
+thv_status thv_serve_wait(thv_server *s, uint64_t ticket, thv_query_stats *st, uint32_t timeout_ms) {
+  if (!s) return fail(THV_EINVAL, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto ready = [&] {
+    auto it = s->queries.find(ticket);
+    return it == s->queries.end() || it->second.done;
+  };
+  if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms ? timeout_ms : 60000), ready))
+    return fail(THV_ETIMEOUT, "query %llu not done", (unsigned long long)ticket);
+  return collect(s, ticket, st);
+}
+
+thv_status thv_serve_stop(thv_server *s) {
+  if (!s) return THV_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stopping = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  const thv_status st = s->fatal;
+  cudaSetDevice(s->g->device);
+  server_free(s);
+  delete s;
+  return st == THV_OK ? THV_OK : fail(st, "server had failed");
+}
+
+}  // extern "C"
