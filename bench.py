@@ -75,6 +75,7 @@ def parse():
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--edge-factor", type=int, default=0, help="override the edge factor")
     ap.add_argument("--rates", default="", help="c5: comma-separated arrival rates (queries/s)")
+    ap.add_argument("--sssp-delta", type=int, default=0, help="c4: batched SSSP window width")
     ap.add_argument("--queries", type=int, default=1024, help="c4: batched sources")
     ap.add_argument("--plain-sample", type=int, default=16, help="c4: single-source runs timed")
     ap.add_argument("--scale", type=int, default=0, help="override the workload's scale")
@@ -353,8 +354,9 @@ def run_batched(args, dist):
         g = T.Graph.generate_rmat(scale, 16, seed=SEED, fmt=fmt, device=dev)
         g.plan(budget if budget is not None else int(args.budget_frac * g.ne * g.esz))
         src = g.pick_sources(args.queries, SEED)
-        g.batch_run(algo, src[:64], want_values=False)  # warm-up
-        _, sums, bst = g.batch_run(algo, src, want_values=False)
+        dl = args.sssp_delta if algo == "sssp" else 0
+        g.batch_run(algo, src[:64], want_values=False, sssp_delta=dl, tune=True)  # tunes, warms up
+        _, sums, bst = g.batch_run(algo, src, want_values=False, sssp_delta=dl, tune=True)
         plain_ms = []
         for s_ in src[: args.plain_sample]:
             vals, st = g.run(algo, source=int(s_))
@@ -364,6 +366,7 @@ def run_batched(args, dist):
         qps_b = dist.n * len(src) / (dist.max(bst["device_ms"]) / 1e3)
         qps_p = dist.n * 1e3 / dist.max(statistics.mean(plain_ms))
         out[algo] = {"batched_qps": qps_b, "plain_qps": qps_p, "speedup": qps_b / qps_p,
+                     "sssp_delta": dl,
                      "batched_ms_total": bst["device_ms"], "plain_ms_mean": statistics.mean(plain_ms),
                      "queries": len(src), "plain_sample": args.plain_sample,
                      "batched_link_bytes": bst["link_edge_bytes"], "batched_iterations": bst["iterations"],

@@ -189,8 +189,12 @@ typedef struct thv_batch_opts {
   void *stream;
   uint32_t small_degree; /* expansion tuning; 0 = autotuned / default */
   uint32_t chunk_edges;  /* expansion tuning; 0 = autotuned / default */
-  uint32_t sssp_delta;   /* shared near/far width for SSSP; 0 = default */
-  uint32_t pad;
+  uint32_t sssp_delta;   /* shared near/far width for SSSP; 0 = 64 */
+  uint32_t tune;         /* 1: without small_degree/chunk_edges, time the
+                            first group under each candidate launch
+                            configuration and keep the fastest (cached per
+                            graph shape in memory and in $THV_TUNE_CACHE or
+                            ~/.cache/thievory_b200_batch_tune.txt) */
 } thv_batch_opts;
 
 /* Runs n sources in groups sharing one traversal each.  out (host, may be

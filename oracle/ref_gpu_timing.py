@@ -27,6 +27,13 @@ CASES = {
 }
 
 
+def is_fixed_point(g, lab):
+    """True if no edge u->w has lab[u] < lab[w] (propagation converged)."""
+    deg = np.diff(g.off.astype(np.int64))
+    src = np.repeat(np.arange(g.nv), deg)
+    return not np.any(lab[src] < lab[g.adj])
+
+
 def main(names, runs=5):
     work = tempfile.mkdtemp()
     os.makedirs(os.path.join(work, "results"))
@@ -51,7 +58,15 @@ def main(names, runs=5):
             res["bit_exact_vs_oracle"] = bool(np.array_equal(vals, want))
         elif c["algo"] == "cc":
             res["traversed"] = g.ne
-            res["bit_exact_vs_oracle"] = bool(np.array_equal(vals, O.cc(g, parallel=True)))
+            want = O.cc(g, parallel=True)
+            res["bit_exact_vs_oracle"] = bool(np.array_equal(vals, want))
+            diff = vals != want
+            res["mismatch"] = {"vertices": int(diff.sum()),
+                               "ref_above_oracle": int((vals > want).sum()),
+                               "ref_below_oracle": int((vals < want).sum()),
+                               "ref_labels": int(len(np.unique(vals))),
+                               "oracle_labels": int(len(np.unique(want))),
+                               "ref_is_fixed_point": bool(is_fixed_point(g, vals))}
         else:
             gw = O.CSR(g.off, g.adj, O.weights(g))
             want = O.sssp(gw, c["src"], parallel=True)

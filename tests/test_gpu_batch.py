@@ -93,3 +93,21 @@ def test_batch_rejects_bad_input(T, O, g14):
 def test_pick_sources_matches_oracle(T, O, g14):
     with T.Graph.from_arrays(g14.off, g14.adj, "csr") as g:
         assert np.array_equal(g.pick_sources(100), O.sources(g14, 100))
+
+
+def test_autotuner_picks_and_caches_a_configuration(T, O, g14, tmp_path, monkeypatch):
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("THV_TUNE_CACHE", str(cache))
+    src = sources(O, g14, 64)
+    with T.Graph.from_arrays(g14.off, g14.adj, "csr") as g:
+        g.plan(int(0.4 * g.ne * 4), block_bytes=BLOCK)
+        out, sums, _ = g.batch_run("bfs", src, tune=True)
+        for i, s in enumerate(src):
+            assert np.array_equal(out[i], O.bfs(g14, int(s)))
+        line = cache.read_text().strip().splitlines()[-1]
+        small, chunk, threads = map(int, line.split("|")[1].split())
+        assert threads in (256, 512) and small >= 16 and chunk >= 128
+        # cached: a second call reuses it (and still matches)
+        out2, sums2, _ = g.batch_run("bfs", src, tune=True)
+        assert np.array_equal(sums, sums2)
+        assert len(cache.read_text().strip().splitlines()) == 1

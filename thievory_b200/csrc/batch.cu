@@ -19,7 +19,13 @@
 // Results are bit-identical to single-source runs: BFS levels are exact
 // (level-synchronous), SSSP is the unique min fixed point.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
 #include <vector>
 
 #include "thv_device.cuh"
@@ -28,7 +34,6 @@
 namespace thv {
 
 enum { MS_BFS = 0, MS_SSSP = 1 };
-constexpr int kMsThreads = 512;
 constexpr uint32_t kMsWidth = 64;       // sources per group (mask bits)
 constexpr uint32_t kMaxBfsLevel = 254;  // u8 level bytes hold level + 1
 
@@ -55,15 +60,14 @@ struct MsArgs {
   unsigned long long *qsm, *qbm;  // masks of the queued items
   unsigned long long cap_s, cap_b;
   MsCtrl *ctrl;
-  const uint32_t *sources;
+  const uint32_t *sources;  // [k, source 0, ..., source k-1]
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, max_iters;
-  uint32_t small_deg, chunk, delta, k;
+  uint32_t small_deg, chunk, delta, pad;
 };
 
 struct BatchState {
   uint64_t nv = 0;
-  uint32_t chunk = 0, small = 0;
   bool sssp = false;
   unsigned long long *d_visit = nullptr, *d_front = nullptr;
   uint8_t *d_lvl = nullptr;
@@ -133,6 +137,64 @@ __device__ __forceinline__ void ms_sssp_edge(const MsArgs &a, uint32_t u, uint32
   }
 }
 
+// Lane-per-source SSSP relaxation of one work item: the warp loads the
+// item's {dst, w} edges 32 at a time (coalesced) and relaxes each edge for
+// every source of the mask at once, lanes = sources, so dist[w][.] is read
+// as coalesced 128-byte lines; four edges' rows are in flight per step.
+__device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t u, uintptr_t eaddr,
+                                             uint32_t cnt, unsigned long long f) {
+  const unsigned lane = lane_id();
+  const bool lo = (f >> lane) & 1ull, hi = (f >> (lane + 32)) & 1ull;
+  const uint32_t *du = a.dist + (size_t)u * kMsWidth;
+  const uint32_t d0 = lo ? ldcg(du + lane) : 0u, d1 = hi ? ldcg(du + 32 + lane) : 0u;
+  for (uint32_t base = 0; base < cnt; base += 32) {
+    const uint32_t k = base + lane;
+    const uint2 e = k < cnt ? ld_nc_u2(eaddr + (uintptr_t)k * 8u) : make_uint2(0, 0);
+    const uint32_t m = min(32u, cnt - base);
+    for (uint32_t j = 0; j < m; j += 4) {
+      uint32_t w[4], wt[4], c0[4], c1[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        w[q] = __shfl_sync(kFull, e.x, (j + q) & 31);
+        wt[q] = __shfl_sync(kFull, e.y, (j + q) & 31);
+        const bool ok = j + q < m;
+        const uint32_t *dw = a.dist + (size_t)w[q] * kMsWidth;
+        c0[q] = ok && lo ? ldcg(dw + lane) : 0u;
+        c1[q] = ok && hi ? ldcg(dw + 32 + lane) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (j + q >= m) break;
+        uint32_t *dw = a.dist + (size_t)w[q] * kMsWidth;
+        bool i0 = false, i1 = false;
+        uint32_t best = 0xFFFFFFFFu;
+        const unsigned long long cd0 = (unsigned long long)d0 + wt[q];
+        const unsigned long long cd1 = (unsigned long long)d1 + wt[q];
+        if (lo && cd0 < c0[q] && cd0 < atomicMin(dw + lane, (uint32_t)cd0)) {
+          i0 = true;
+          best = (uint32_t)cd0;
+        }
+        if (hi && cd1 < c1[q] && cd1 < atomicMin(dw + 32 + lane, (uint32_t)cd1)) {
+          i1 = true;
+          best = min(best, (uint32_t)cd1);
+        }
+        const unsigned b0 = __ballot_sync(kFull, i0), b1 = __ballot_sync(kFull, i1);
+        if (b0 | b1) {
+          best = warp_min(best);
+          if (lane == 0) {
+            atomicOr(a.front + w[q], (unsigned long long)b0 | ((unsigned long long)b1 << 32));
+            atomicMin(a.wmin + (w[q] >> 5), best);
+            mark_pending<MS_SSSP>(a, w[q]);
+          }
+        }
+      }
+    }
+  }
+}
+
+// masks with at most this many sources relax lane-per-edge instead
+constexpr int kSparseMask = 4;
+
 template <int OP, int ESZ>
 __device__ __forceinline__ void ms_edge(const MsArgs &a, uint32_t u, uint32_t w,
                                         uint32_t wt, unsigned long long f, uint32_t lvl1) {
@@ -143,6 +205,10 @@ __device__ __forceinline__ void ms_edge(const MsArgs &a, uint32_t u, uint32_t w,
 template <int OP, int ESZ>
 __device__ __forceinline__ void ms_chunk(const MsArgs &a, const WorkItem &it,
                                          unsigned long long f, uint32_t lvl1) {
+  if (OP == MS_SSSP && __popcll(f) > kSparseMask) {
+    ms_sssp_item(a, it.v, it.eaddr, it.cnt, f);
+    return;
+  }
   constexpr int PER = 16 / ESZ;
   const unsigned lane = lane_id();
   const uintptr_t start = it.eaddr;
@@ -170,6 +236,20 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long fir
     it = a.qs[idx];
     f = a.qsm[idx];
   }
+  if (OP == MS_SSSP) {
+    // items with dense masks: one at a time, lanes = sources
+    unsigned dense = __ballot_sync(kFull, __popcll(f) > kSparseMask);
+    while (dense) {
+      const int i = __ffs(dense) - 1;
+      dense &= dense - 1;
+      ms_sssp_item(a, __shfl_sync(kFull, it.v, i), (uintptr_t)shfl64(it.eaddr, i),
+                   __shfl_sync(kFull, it.cnt, i), shfl64(f, i));
+    }
+    if (__popcll(f) > kSparseMask) {
+      it.cnt = 0;
+      f = 0;
+    }
+  }
   const unsigned incl = warp_incl_scan<unsigned>(it.cnt);
   const unsigned excl = incl - it.cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
@@ -192,8 +272,8 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long fir
   }
 }
 
-template <int OP, int ESZ>
-__global__ void __launch_bounds__(kMsThreads) ms_kernel(MsArgs a) {
+template <int OP, int ESZ, int THREADS>
+__global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
   extern __shared__ uint32_t s_vb[];
   const bool smem_tab = a.nblk <= kSmemBlocks;
   if (smem_tab)
@@ -401,8 +481,8 @@ __global__ void ms_init(MsArgs a, uint32_t nw_alloc) {
 template <int OP>
 __global__ void ms_seed(MsArgs a) {
   const uint32_t s = threadIdx.x;
-  if (s >= a.k) return;
-  const uint32_t v = a.sources[s];
+  if (s >= a.sources[0]) return;
+  const uint32_t v = a.sources[1 + s];
   atomicOr(a.front + v, 1ull << s);
   atomicOr(a.bm + (v >> 5), 1u << (v & 31u));
   if (OP == MS_BFS) {
@@ -428,6 +508,7 @@ template <int OP>
 __global__ void ms_extract(MsArgs a, uint32_t *out, unsigned long long *sums) {
   __shared__ unsigned long long s_sum[kMsWidth];
   __shared__ uint32_t tile[32][kMsWidth + 1];
+  const uint32_t k = a.sources[0];
   for (uint32_t i = threadIdx.x; i < kMsWidth; i += blockDim.x) s_sum[i] = 0;
   __syncthreads();
   const uint32_t inf = a.nv + 1u;
@@ -451,7 +532,7 @@ __global__ void ms_extract(MsArgs a, uint32_t *out, unsigned long long *sums) {
     for (uint32_t i = threadIdx.x; i < 32 * kMsWidth; i += blockDim.x) {
       const uint32_t s = i / 32, dv = i % 32;
       const uint64_t v = base + dv;
-      if (s < a.k && v < a.nv) {
+      if (s < k && v < a.nv) {
         const uint32_t val = tile[dv][s];
         if (out) out[(uint64_t)s * a.nv + v] = val;
         if (sums) atomicAdd(&s_sum[s], value_hash((uint32_t)v, val));
@@ -460,15 +541,57 @@ __global__ void ms_extract(MsArgs a, uint32_t *out, unsigned long long *sums) {
     __syncthreads();
   }
   if (sums)
-    for (uint32_t i = threadIdx.x; i < a.k; i += blockDim.x)
+    for (uint32_t i = threadIdx.x; i < k; i += blockDim.x)
       if (s_sum[i]) atomicAdd(sums + i, s_sum[i]);
 }
 
 // ------------------------------------------------------------------ host --
 
+// Launch configuration of the batch kernel: the degree-bucket boundary
+// (below: 32 vertices per warp, one thread per vertex with warp-cooperative
+// load balancing; at or above: chunks of `chunk` edges per warp) and the
+// threads per CTA.
+struct MsConfig {
+  uint32_t small, chunk, threads;
+  bool operator<(const MsConfig &o) const {
+    return std::tie(small, chunk, threads) < std::tie(o.small, o.chunk, o.threads);
+  }
+};
+
+constexpr MsConfig kMsDefault{64, 256, 512};
+// candidates the autotuner times (one real group each)
+const MsConfig kMsCandidates[] = {{16, 128, 512}, {64, 256, 512}, {256, 512, 512},
+                                  {64, 1024, 512}, {16, 128, 256}, {64, 256, 256},
+                                  {256, 512, 256}, {64, 1024, 256}};
+constexpr uint32_t kMsMinSmall = 16, kMsMinChunk = 128;
+
+struct GraphKey {
+  int op, esz, threads;
+  bool out;
+  uint32_t small, chunk;
+  bool operator<(const GraphKey &o) const {
+    return std::tie(op, esz, threads, out, small, chunk) <
+           std::tie(o.op, o.esz, o.threads, o.out, o.small, o.chunk);
+  }
+};
+
+struct BatchExtra {
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  bool capture_ok = true;
+};
+
+static std::map<BatchState *, BatchExtra> g_extra;  // graphs per batch state
+static std::mutex g_tune_mu;
+static std::map<std::string, MsConfig> g_tune;     // in-process tuner cache
+
 void batch_free(thv_graph *g) {
   BatchState *b = g->bs;
   if (!b) return;
+  auto it = g_extra.find(b);
+  if (it != g_extra.end()) {
+    for (auto &kv : it->second.graphs) cudaGraphExecDestroy(kv.second);
+    g_extra.erase(it);
+  }
   dev_free(b->d_visit);
   dev_free(b->d_front);
   dev_free(b->d_lvl);
@@ -492,23 +615,20 @@ void batch_free(thv_graph *g) {
   g->bs = nullptr;
 }
 
-static thv_status ensure_batch_state(thv_graph *g, bool sssp, uint32_t chunk,
-                                     uint32_t small, bool want_out) {
+// Queues are sized for the smallest bucket boundary and chunk any
+// configuration may use, so tuning never reallocates.
+static thv_status ensure_batch_state(thv_graph *g, bool sssp, bool want_out) {
   BatchState *&b = g->bs;
-  if (b && b->sssp == sssp && b->chunk == chunk && b->small == small &&
-      (!want_out || b->d_out))
-    return THV_OK;
+  if (b && b->sssp == sssp && (!want_out || b->d_out)) return THV_OK;
   batch_free(g);
   b = new BatchState();
   b->nv = g->nv;
   b->sssp = sssp;
-  b->chunk = chunk;
-  b->small = small;
   const uint64_t nw = (g->nv + 31) / 32;
   b->ngroups = (uint32_t)((nw + 31) / 32);
   const uint64_t nw_alloc = (uint64_t)b->ngroups * 32;
   b->cap_s = g->nv + 32;
-  b->cap_b = g->ne / chunk + g->ne / std::max<uint32_t>(small, 1) + 64;
+  b->cap_b = g->ne / kMsMinChunk + g->ne / kMsMinSmall + 64;
   THV_TRY(dev_alloc((void **)&b->d_front, g->nv * 8 + 64, "batch frontier masks"));
   if (sssp) {
     THV_TRY(dev_alloc((void **)&b->d_dist, g->nv * kMsWidth * 4 + 64, "batch distances"));
@@ -524,8 +644,8 @@ static thv_status ensure_batch_state(thv_graph *g, bool sssp, uint32_t chunk,
   THV_TRY(dev_alloc((void **)&b->d_qbm, b->cap_b * 8, "batch chunk masks"));
   THV_TRY(dev_alloc((void **)&b->d_ctrl, sizeof(MsCtrl), "batch control"));
   THV_TRY(pinned_alloc((void **)&b->h_ctrl, sizeof(MsCtrl), "batch control"));
-  THV_TRY(dev_alloc((void **)&b->d_sources, kMsWidth * 4, "batch sources"));
-  THV_TRY(pinned_alloc((void **)&b->h_sources, kMsWidth * 4, "batch sources"));
+  THV_TRY(dev_alloc((void **)&b->d_sources, (kMsWidth + 1) * 4, "batch sources"));
+  THV_TRY(pinned_alloc((void **)&b->h_sources, (kMsWidth + 1) * 4, "batch sources"));
   THV_TRY(dev_alloc((void **)&b->d_sums, kMsWidth * 8, "batch checksums"));
   THV_TRY(pinned_alloc((void **)&b->h_sums, kMsWidth * 8, "batch checksums"));
   if (want_out) THV_TRY(dev_alloc((void **)&b->d_out, (uint64_t)kMsWidth * g->nv * 4 + 64, "batch output"));
@@ -534,27 +654,78 @@ static thv_status ensure_batch_state(thv_graph *g, bool sssp, uint32_t chunk,
   return THV_OK;
 }
 
-template <int OP, int ESZ>
-static thv_status launch_group(thv_graph *g, MsArgs &a, cudaStream_t st, bool want_out,
-                               uint32_t &launches) {
+// The whole group -- sources up, reset, seed, persistent traversal,
+// extraction, status down -- enqueued on `st` (captured into a graph once).
+template <int OP, int ESZ, int THREADS>
+static thv_status enqueue_group(thv_graph *g, MsArgs &a, cudaStream_t st, bool want_out) {
   BatchState *b = g->bs;
-  auto kern = ms_kernel<OP, ESZ>;
+  auto kern = ms_kernel<OP, ESZ, THREADS>;
   const size_t smem = g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0;
   int bpsm = 0;
-  THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kMsThreads, smem));
+  THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, THREADS, smem));
   if (bpsm < 1) return fail(THV_ECUDA, "batch kernel cannot be resident");
   const int grid = bpsm * g->num_sms;
   const int igrid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 255) / 256)));
-  THV_CUDA(cudaMemcpyAsync(b->d_sources, b->h_sources, kMsWidth * 4, cudaMemcpyHostToDevice, st));
+  THV_CUDA(cudaMemcpyAsync(b->d_sources, b->h_sources, (kMsWidth + 1) * 4, cudaMemcpyHostToDevice, st));
   ms_init<OP><<<igrid, 256, 0, st>>>(a, b->ngroups * 32u);
   ms_seed<OP><<<1, kMsWidth, 0, st>>>(a);
-  THV_CUDA(cudaGetLastError());
   void *args[] = {&a};
-  THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(kMsThreads), args, smem, st));
+  THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(THREADS), args, smem, st));
   THV_CUDA(cudaMemsetAsync(b->d_sums, 0, kMsWidth * 8, st));
   const int xgrid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 31) / 32)));
   ms_extract<OP><<<xgrid, 256, 0, st>>>(a, want_out ? b->d_out : nullptr, b->d_sums);
+  THV_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, sizeof(MsCtrl), cudaMemcpyDeviceToHost, st));
+  THV_CUDA(cudaMemcpyAsync(b->h_sums, b->d_sums, kMsWidth * 8, cudaMemcpyDeviceToHost, st));
   THV_CUDA(cudaGetLastError());
+  return THV_OK;
+}
+
+template <int OP, int ESZ>
+static thv_status enqueue_any(thv_graph *g, MsArgs &a, cudaStream_t st, bool want_out,
+                              uint32_t threads) {
+  return threads == 256 ? enqueue_group<OP, ESZ, 256>(g, a, st, want_out)
+                        : enqueue_group<OP, ESZ, 512>(g, a, st, want_out);
+}
+
+static thv_status enqueue(thv_graph *g, bool sssp, MsArgs &a, cudaStream_t st, bool want_out,
+                          uint32_t threads) {
+  if (sssp) {
+    if (g->esz != 8) return fail(THV_EINVAL, "SSSP needs 8-byte weighted edges");
+    return enqueue_any<MS_SSSP, 8>(g, a, st, want_out, threads);
+  }
+  return g->esz == 8 ? enqueue_any<MS_BFS, 8>(g, a, st, want_out, threads)
+                     : enqueue_any<MS_BFS, 4>(g, a, st, want_out, threads);
+}
+
+// Runs the group whose sources sit in h_sources; replays a captured CUDA
+// graph of the launch sequence when capture works on this stream.
+static thv_status run_group(thv_graph *g, bool sssp, MsArgs &a, cudaStream_t st, bool want_out,
+                            const MsConfig &cfg, uint32_t &launches) {
+  BatchState *b = g->bs;
+  BatchExtra &ex = g_extra[b];
+  const GraphKey key{sssp ? 1 : 0, (int)g->esz, (int)cfg.threads, want_out, cfg.small, cfg.chunk};
+  auto it = ex.graphs.find(key);
+  if (it == ex.graphs.end() && ex.capture_ok) {
+    cudaStream_t cs = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    thv_status s = ok ? enqueue(g, sssp, a, cs, want_out, cfg.threads) : THV_ECUDA;
+    if (ok) ok = cudaStreamEndCapture(cs, &graph) == cudaSuccess && s == THV_OK;
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (cs) cudaStreamDestroy(cs);
+    cudaGetLastError();
+    if (ok) it = ex.graphs.emplace(key, exec).first;
+    else ex.capture_ok = false;  // fall back to direct launches from now on
+  }
+  if (it != ex.graphs.end()) {
+    THV_CUDA(cudaGraphLaunch(it->second, st));
+    launches += 4;
+    return THV_OK;
+  }
+  THV_TRY(enqueue(g, sssp, a, st, want_out, cfg.threads));
   launches += 4;
   return THV_OK;
 }
@@ -593,6 +764,60 @@ static thv_status fallback_single(thv_graph *g, const uint32_t *src, uint32_t k,
   return THV_OK;
 }
 
+static std::string tune_key(const thv_graph *g, bool sssp) {
+  char buf[160];
+  snprintf(buf, sizeof(buf), "%s nv=%llu ne=%llu esz=%u resident=%llu blocks=%zu sms=%d",
+           sssp ? "sssp" : "bfs", (unsigned long long)g->nv, (unsigned long long)g->ne, g->esz,
+           (unsigned long long)g->plan.resident_edge_bytes, g->plan.blocks.size(), g->num_sms);
+  return buf;
+}
+
+static std::string tune_file() {
+  const char *p = getenv("THV_TUNE_CACHE");
+  if (p && *p) return p;
+  const char *h = getenv("HOME");
+  return std::string(h && *h ? h : "/tmp") + "/.cache/thievory_b200_batch_tune.txt";
+}
+
+static bool tune_lookup(const std::string &key, MsConfig *cfg) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(key);
+  if (it != g_tune.end()) { *cfg = it->second; return true; }
+  FILE *f = fopen(tune_file().c_str(), "r");
+  if (!f) return false;
+  char line[512];
+  bool found = false;
+  while (fgets(line, sizeof(line), f)) {
+    char *bar = strchr(line, '|');
+    if (!bar) continue;
+    *bar = 0;
+    MsConfig c{};
+    if (key == line && sscanf(bar + 1, "%u %u %u", &c.small, &c.chunk, &c.threads) == 3 &&
+        (c.threads == 256 || c.threads == 512) && c.small >= kMsMinSmall && c.chunk >= kMsMinChunk) {
+      *cfg = c;
+      found = true;
+    }
+  }
+  fclose(f);
+  if (found) g_tune[key] = *cfg;
+  return found;
+}
+
+static void tune_store(const std::string &key, const MsConfig &c) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = c;
+  const std::string path = tune_file();
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos) {
+    std::string dir = path.substr(0, slash);
+    (void)!system(("mkdir -p '" + dir + "' 2>/dev/null").c_str());
+  }
+  FILE *f = fopen(path.c_str(), "a");
+  if (!f) return;
+  fprintf(f, "%s|%u %u %u\n", key.c_str(), c.small, c.chunk, c.threads);
+  fclose(f);
+}
+
 thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
                      uint32_t n, const thv_batch_opts *o, uint32_t *out,
                      uint64_t *checksums, thv_stats *stats) {
@@ -607,10 +832,7 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
   const uint32_t group = o && o->group ? std::min<uint32_t>(o->group, kMsWidth) : kMsWidth;
   const double t0 = now_ms();
   THV_TRY(ensure_plan(g));
-  uint32_t small = 64, chunk = 256;
-  if (o && o->small_degree) small = o->small_degree;
-  if (o && o->chunk_edges) chunk = std::max<uint32_t>(32, (o->chunk_edges + 31) / 32 * 32);
-  THV_TRY(ensure_batch_state(g, sssp, chunk, small, out != nullptr));
+  THV_TRY(ensure_batch_state(g, sssp, out != nullptr));
   BatchState *b = g->bs;
   cudaStream_t st = o && o->stream ? (cudaStream_t)o->stream : g->stream;
   MsArgs a{};
@@ -638,52 +860,81 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
   a.nv = (uint32_t)g->nv;
   a.ngroups = b->ngroups;
   a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0x7FFFFFF0ull) * 2 + 8;
-  a.small_deg = small;
-  a.chunk = chunk;
-  a.delta = o && o->sssp_delta ? o->sssp_delta : 2u;
+  // 64: many sources expand a vertex in the same iteration and share its
+  // adjacency read (small windows make each source re-read it)
+  a.delta = o && o->sssp_delta ? o->sssp_delta : 64u;
+
   thv_stats local{};
   uint32_t launches = 0;
   float dev_ms = 0.f;
-  for (uint32_t first = 0; first < n; first += group) {
-    const uint32_t k = std::min(group, n - first);
-    a.k = k;
-    memcpy(b->h_sources, sources + first, k * 4);
+  auto set_cfg = [&](const MsConfig &c) {
+    a.small_deg = std::max(c.small, kMsMinSmall);
+    a.chunk = std::max(c.chunk, kMsMinChunk);
+  };
+  auto one_group = [&](uint32_t first, uint32_t k, const MsConfig &cfg, float *ms_out,
+                       bool *deep) -> thv_status {
+    set_cfg(cfg);
+    b->h_sources[0] = k;
+    memcpy(b->h_sources + 1, sources + first, k * 4);
     THV_CUDA(cudaEventRecord(b->ev0, st));
-    thv_status s = g->esz == 8
-        ? (sssp ? launch_group<MS_SSSP, 8>(g, a, st, out != nullptr, launches)
-                : launch_group<MS_BFS, 8>(g, a, st, out != nullptr, launches))
-        : (sssp ? fail(THV_EINVAL, "SSSP needs 8-byte weighted edges")
-                : launch_group<MS_BFS, 4>(g, a, st, out != nullptr, launches));
-    if (s != THV_OK) return s;
+    THV_TRY(run_group(g, sssp, a, st, out != nullptr, cfg, launches));
     THV_CUDA(cudaEventRecord(b->ev1, st));
-    THV_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, sizeof(MsCtrl), cudaMemcpyDeviceToHost, st));
-    THV_CUDA(cudaMemcpyAsync(b->h_sums, b->d_sums, kMsWidth * 8, cudaMemcpyDeviceToHost, st));
     if (out)
       THV_CUDA(cudaMemcpyAsync(out + (uint64_t)first * g->nv, b->d_out, (uint64_t)k * g->nv * 4,
                                cudaMemcpyDeviceToHost, st));
     THV_CUDA(cudaStreamSynchronize(st));
-    float ms_ = 0.f;
-    cudaEventElapsedTime(&ms_, b->ev0, b->ev1);
-    dev_ms += ms_;
+    cudaEventElapsedTime(ms_out, b->ev0, b->ev1);
     const MsCtrl &hc = *b->h_ctrl;
-    if (hc.err == kDevErrDepth) {
-      // deeper than the u8 level bytes hold: run this group one source at a time
+    *deep = hc.err == kDevErrDepth;
+    if (hc.err == kDevErrBarrier) return fail(THV_ETIMEOUT, "grid barrier wait exceeded %u ms", tmo);
+    if (hc.err == kDevErrIters) return fail(THV_ETIMEOUT, "iteration cap reached");
+    if (hc.err && hc.err != kDevErrDepth) return fail(THV_EDEVICE, "batch device error %u", hc.err);
+    return THV_OK;
+  };
+
+  // configuration: explicit, cached, autotuned on the first group, or default
+  MsConfig cfg = kMsDefault;
+  if (o && (o->small_degree || o->chunk_edges)) {
+    cfg.small = o->small_degree ? o->small_degree : kMsDefault.small;
+    cfg.chunk = o->chunk_edges ? std::max<uint32_t>(32, (o->chunk_edges + 31) / 32 * 32) : kMsDefault.chunk;
+  } else {
+    const std::string key = tune_key(g, sssp);
+    if (!tune_lookup(key, &cfg) && o && o->tune && n > 0) {
+      const uint32_t k = std::min(group, n);
+      float best_ms = 1e30f;
+      for (const MsConfig &c : kMsCandidates) {
+        float ms_ = 0;
+        bool deep = false;
+        THV_TRY(one_group(0, k, c, &ms_, &deep));
+        if (deep) break;  // depth fallback: tuning this graph is moot
+        if (ms_ < best_ms) { best_ms = ms_; cfg = c; }
+      }
+      tune_store(key, cfg);
+    }
+  }
+
+  for (uint32_t first = 0; first < n; first += group) {
+    const uint32_t k = std::min(group, n - first);
+    float ms_ = 0.f;
+    bool deep = false;
+    THV_TRY(one_group(first, k, cfg, &ms_, &deep));
+    if (deep) {
+      // deeper than the u8 level bytes hold: this group one source at a time
       THV_TRY(fallback_single(g, sources + first, k, st, o, out ? out + (uint64_t)first * g->nv : nullptr,
                               checksums ? checksums + first : nullptr, local));
       continue;
     }
-    if (hc.err == kDevErrBarrier) return fail(THV_ETIMEOUT, "grid barrier wait exceeded %u ms", tmo);
-    if (hc.err == kDevErrIters) return fail(THV_ETIMEOUT, "iteration cap reached");
-    if (hc.err) return fail(THV_EDEVICE, "batch device error %u", hc.err);
+    dev_ms += ms_;
+    const MsCtrl &hc = *b->h_ctrl;
     if (checksums) memcpy(checksums + first, b->h_sums, k * 8);
     local.iterations += hc.iters;
     local.edges_expanded += hc.edges;
     local.hbm_edge_bytes += hc.hbm_bytes;
     local.link_edge_bytes += hc.link_bytes;
-    local.h2d_bytes += kMsWidth * 4;
+    local.h2d_bytes += (kMsWidth + 1) * 4;
     local.d2h_bytes += sizeof(MsCtrl) + kMsWidth * 8 + (out ? (uint64_t)k * g->nv * 4 : 0);
   }
-  local.device_ms = dev_ms;
+  local.device_ms += dev_ms;
   local.kernel_launches = launches;
   local.wall_ms = now_ms() - t0;
   if (stats) *stats = local;

@@ -50,6 +50,21 @@ constexpr uint32_t kDefaultDelta = 2;   // SSSP near/far width (weights >= 1)
 constexpr uint32_t kCcGrowth = 8;       // CC label window growth per advance
 
 
+// Frontier work item of the single-source engine: the adjacency of vertex v
+// (or one chunk of it) plus v's value when it was taken, so the expansion
+// needs no dependent load of val[v] (a value that fell since is a larger,
+// still valid bound, and the fall re-queued v).  Edge addresses fit in 48
+// bits (checked on the host); the edge count takes the top 16.
+struct __align__(16) MinItem {
+  unsigned long long ea_cnt;
+  uint32_t v, val;
+};
+constexpr unsigned long long kAddrMask = (1ull << 48) - 1;
+__device__ __forceinline__ MinItem make_item(unsigned long long ea, uint32_t cnt, uint32_t v,
+                                             uint32_t val) {
+  return MinItem{ea | ((unsigned long long)cnt << 48), v, val};
+}
+
 struct MinCtrl {
   GridBar bar;
   unsigned err, iters;
@@ -67,7 +82,7 @@ struct MinArgs {
   const uint32_t *blk_vb;
   const uint64_t *blk_base;
   uint64_t host_base;
-  WorkItem *qs, *qb;
+  MinItem *qs, *qb;
   unsigned long long cap_s, cap_b;
   MinCtrl *ctrl;
   unsigned long long timeout_ns;
@@ -81,7 +96,7 @@ struct MinState {
   uint32_t *d_val = nullptr;
   uint32_t *d_bm = nullptr;
   uint32_t *d_wmin = nullptr;
-  WorkItem *d_qs = nullptr, *d_qb = nullptr;
+  MinItem *d_qs = nullptr, *d_qb = nullptr;
   uint64_t cap_s = 0, cap_b = 0;
   uint32_t chunk = 0, small = 0;
   MinCtrl *d_ctrl = nullptr;
@@ -128,12 +143,12 @@ __device__ __forceinline__ unsigned long long candidate(uint32_t vval, uint32_t 
 // One high-degree chunk per warp: 128-byte aligned 16-byte loads, two per
 // lane in flight, lanes outside [start, end) masked.
 template <int OP, int ESZ>
-__device__ __forceinline__ void process_chunk(const MinArgs &a, const WorkItem &it) {
+__device__ __forceinline__ void process_chunk(const MinArgs &a, const MinItem &it) {
   constexpr int PER = 16 / ESZ;  // edges per 16-byte load
   const unsigned lane = lane_id();
-  const uint32_t vval = ldcg(a.val + it.v);
-  const uintptr_t start = it.eaddr;
-  const uintptr_t end = start + (uintptr_t)it.cnt * ESZ;
+  const uint32_t vval = it.val;
+  const uintptr_t start = it.ea_cnt & kAddrMask;
+  const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
   for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end; p += 1024u) {
     uint4 q[2];
     q[0] = ld_nc_v4(p);
@@ -166,14 +181,13 @@ __device__ __forceinline__ void process_group(const MinArgs &a, unsigned long lo
                               unsigned long long n_small) {
   const unsigned lane = lane_id();
   const unsigned long long idx = first + lane;
-  WorkItem it{0, 0, 0};
-  uint32_t vval = 0;
-  if (idx < n_small) {
-    it = a.qs[idx];
-    vval = ldcg(a.val + it.v);
-  }
-  const unsigned incl = warp_incl_scan<unsigned>(it.cnt);
-  const unsigned excl = incl - it.cnt;
+  MinItem it{0, 0, 0};
+  if (idx < n_small) it = a.qs[idx];
+  const uint32_t vval = it.val;
+  const unsigned cnt = (unsigned)(it.ea_cnt >> 48);
+  const unsigned long long eaddr = it.ea_cnt & kAddrMask;
+  const unsigned incl = warp_incl_scan<unsigned>(cnt);
+  const unsigned excl = incl - cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
   for (unsigned k = 0; k < total; k += 64) {
     uint32_t w[2];
@@ -185,7 +199,7 @@ __device__ __forceinline__ void process_group(const MinArgs &a, unsigned long lo
     for (int h = 0; h < 2; h++) {
       const unsigned t = k + 32u * h + lane;
       const int o = warp_owner(excl, t);
-      const unsigned long long ea = shfl64(it.eaddr, o);
+      const unsigned long long ea = shfl64(eaddr, o);
       const unsigned oex = __shfl_sync(kFull, excl, o);
       ov[h] = __shfl_sync(kFull, vval, o);
       ok[h] = t < total;
@@ -211,13 +225,18 @@ __device__ __forceinline__ void process_group(const MinArgs &a, unsigned long lo
 template <int OP, int ESZ>
 __global__ void __launch_bounds__(kMinThreads)
     minprop_kernel(MinArgs a) {
-  extern __shared__ uint32_t s_vb[];
+  // block table (first vertex, base address) in shared memory when it fits
+  extern __shared__ unsigned long long s_tab[];
   const bool smem_tab = a.nblk <= kSmemBlocks;
-  if (smem_tab)
-    for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x)
-      s_vb[i] = a.blk_vb[i];
+  unsigned long long *s_base = s_tab;
+  uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_tab + a.nblk);
+  if (smem_tab) {
+    for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x) s_vb[i] = a.blk_vb[i];
+    for (uint32_t i = threadIdx.x; i < a.nblk; i += blockDim.x) s_base[i] = a.blk_base[i];
+  }
   __syncthreads();
   const uint32_t *vb = smem_tab ? s_vb : a.blk_vb;
+  const unsigned long long *bbase = smem_tab ? s_base : (const unsigned long long *)a.blk_base;
   MinCtrl *c = a.ctrl;
   const unsigned lane = lane_id();
   const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -291,10 +310,10 @@ __global__ void __launch_bounds__(kMinThreads)
         uint32_t deg = 0;
         unsigned long long eaddr = 0;
         if (take) {
+          if (OP == OP_BFS) vval = ldcg(a.val + v);
           const uint64_t s = __ldg(a.off + v), e = __ldg(a.off + v + 1);
           deg = (uint32_t)(e - s);
-          const uint32_t b = find_block(vb, a.nblk, v);
-          const unsigned long long base = __ldg(a.blk_base + b);
+          const unsigned long long base = bbase[find_block(vb, a.nblk, v)];
           eaddr = base + s * ESZ;
           my_edges += deg;
           my_verts += 1;
@@ -312,7 +331,7 @@ __global__ void __launch_bounds__(kMinThreads)
           base = shfl64(base, ldr);
           const unsigned long long pos = base + __popc(sm & lanemask_lt());
           if (small) {
-            if (pos < a.cap_s) a.qs[pos] = WorkItem{eaddr, v, deg};
+            if (pos < a.cap_s) a.qs[pos] = make_item(eaddr, deg, v, vval);
             else atomicCAS(&c->err, 0u, kDevErrQueue);
           }
         }
@@ -329,7 +348,7 @@ __global__ void __launch_bounds__(kMinThreads)
               const uint32_t lo = k * a.chunk;
               const uint32_t cnt = min(a.chunk, deg - lo);
               if (pos < a.cap_b)
-                a.qb[pos] = WorkItem{eaddr + (unsigned long long)lo * ESZ, v, cnt};
+                a.qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, cnt, v, vval);
               else
                 atomicCAS(&c->err, 0u, kDevErrQueue);
             }
@@ -373,15 +392,16 @@ __global__ void __launch_bounds__(kMinThreads)
     // all for warps without a first task)
     const unsigned long long ntask = nb + (ns + 31) / 32;
     for (unsigned long long t = gwarp; t < ntask;) {
+      // reserve the next task before working on this one (latency overlap)
+      unsigned long long nt = 0;
+      if (lane == 0) nt = atomicAdd(&c->wc[slot], 1ull);
       if (t < nb) {
-        const WorkItem it = a.qb[t];
+        const MinItem it = a.qb[t];
         process_chunk<OP, ESZ>(a, it);
       } else {
         process_group<OP, ESZ>(a, (t - nb) * 32ull, ns);
       }
-      unsigned long long nt = 0;
-      if (lane == 0) nt = nwarps + atomicAdd(&c->wc[slot], 1ull);
-      t = shfl64(nt, 0);
+      t = nwarps + shfl64(nt, 0);
     }
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
   }
@@ -462,8 +482,8 @@ static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
   THV_TRY(dev_alloc((void **)&ms->d_val, g->nv * 4 + 64, "values"));
   THV_TRY(dev_alloc((void **)&ms->d_bm, nw_alloc * 4, "pending bitmap"));
   THV_TRY(dev_alloc((void **)&ms->d_wmin, nw_alloc * 4, "pending minima"));
-  THV_TRY(dev_alloc((void **)&ms->d_qs, ms->cap_s * sizeof(WorkItem), "queue"));
-  THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(WorkItem), "chunk queue"));
+  THV_TRY(dev_alloc((void **)&ms->d_qs, ms->cap_s * sizeof(MinItem), "queue"));
+  THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(MinItem), "chunk queue"));
   THV_TRY(dev_alloc((void **)&ms->d_ctrl, sizeof(MinCtrl), "control"));
   THV_TRY(pinned_alloc((void **)&ms->h_ctrl, sizeof(MinCtrl), "control"));
   THV_CUDA(cudaEventCreate(&ms->ev0));
@@ -492,8 +512,8 @@ template <int OP, int ESZ>
 static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
                                  uint32_t &launches) {
   auto kern = minprop_kernel<OP, ESZ>;
-  const size_t smem =
-      g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0;
+  const size_t nb = g->plan.blocks.size();
+  const size_t smem = nb <= kSmemBlocks ? nb * 8 + (nb + 1) * 4 : 0;
   int bpsm = 0;
   THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern,
                                                          kMinThreads, smem));
@@ -527,9 +547,14 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
     return fail(THV_EINVAL, "source %u out of range (n=%llu)", src,
                 (unsigned long long)g->nv);
   uint32_t chunk = o && o->chunk_edges ? o->chunk_edges : kDefaultChunk;
-  chunk = std::max<uint32_t>(32, (chunk + 31) / 32 * 32);
-  const uint32_t small = o && o->small_degree ? o->small_degree : kDefaultSmall;
+  chunk = std::min<uint32_t>(32768, std::max<uint32_t>(32, (chunk + 31) / 32 * 32));
+  const uint32_t small =
+      std::min<uint32_t>(32768, o && o->small_degree ? o->small_degree : kDefaultSmall);
   THV_TRY(ensure_plan(g));
+  // work items keep edge addresses in 48 bits
+  const uint64_t top = std::max<uint64_t>(g->h_edges_dev + g->h_edges_bytes,
+                                          (uint64_t)g->plan.d_resident + g->plan.d_resident_bytes);
+  if (top >> 48) return fail(THV_EUNSUPPORTED, "edge address above 2^48");
   THV_TRY(ensure_min_state(g, chunk, small));
   MinState *ms = g->ms;
 

@@ -9,7 +9,8 @@
 // zero-copy addressing), with per-slot near/far thresholds so that queries
 // admitted at different times coexist.  BFS slots relax with unit weights
 // (distance + 1 == level + 1, window 1: exactly level-synchronous); SSSP
-// slots use the edge weights with window 2.
+// slots use the edge weights with window 64: wide enough that many slots
+// expand the same vertex in the same iteration and share its edge read.
 //
 // The persistent kernel returns to the host when any slot's query has no
 // pending vertex left, or after a bounded number of iterations when
@@ -20,6 +21,7 @@
 // launch boundary and shares every later edge read with them.
 #include <algorithm>
 #include <chrono>
+#include <cstddef>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -35,7 +37,7 @@ namespace thv {
 
 constexpr int kSvThreads = 512;
 constexpr uint32_t kSvMaxSlots = 64;
-constexpr uint32_t kSvDeltaSssp = 2;
+constexpr uint32_t kSvDeltaSssp = 64;  // shared-read sweet spot (batched sweep)
 
 struct SvCtrl {
   GridBar bar;
@@ -94,8 +96,70 @@ __device__ __forceinline__ void sv_edge(const SvArgs &a, uint32_t u, uint32_t w,
   }
 }
 
+// Lane-per-slot relaxation of one work item (dense masks): edges loaded 32
+// at a time, each relaxed for all slots of the mask at once with lanes =
+// slots, so val[w][.] is read as coalesced lines; four rows in flight.
+template <int ESZ>
+__device__ __forceinline__ void sv_item_rows(const SvArgs &a, uint32_t u, uintptr_t eaddr,
+                                             uint32_t cnt, unsigned long long f) {
+  const unsigned lane = lane_id();
+  const bool lo = (f >> lane) & 1ull, hi = (f >> (lane + 32)) & 1ull;
+  const uint32_t one0 = (uint32_t)((a.unit >> lane) & 1ull);
+  const uint32_t one1 = (uint32_t)((a.unit >> (lane + 32)) & 1ull);
+  const uint32_t *du = a.val + (size_t)u * a.W;
+  const uint32_t d0 = lo ? ldcg(du + lane) : 0u, d1 = hi ? ldcg(du + 32 + lane) : 0u;
+  for (uint32_t base = 0; base < cnt; base += 32) {
+    const uint32_t k = base + lane;
+    uint32_t ex = 0, ey = 1;
+    if (k < cnt) {
+      if (ESZ == 4) {
+        ex = ld_nc_u32(eaddr + (uintptr_t)k * 4u);
+      } else {
+        const uint2 e = ld_nc_u2(eaddr + (uintptr_t)k * 8u);
+        ex = e.x;
+        ey = e.y;
+      }
+    }
+    const uint32_t m = min(32u, cnt - base);
+    for (uint32_t j = 0; j < m; j += 4) {
+      uint32_t w[4], wt[4], c0[4], c1[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        w[q] = __shfl_sync(kFull, ex, (j + q) & 31);
+        wt[q] = __shfl_sync(kFull, ey, (j + q) & 31);
+        const bool ok = j + q < m;
+        const uint32_t *dw = a.val + (size_t)w[q] * a.W;
+        c0[q] = ok && lo ? ldcg(dw + lane) : 0u;
+        c1[q] = ok && hi ? ldcg(dw + 32 + lane) : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        if (j + q >= m) break;
+        uint32_t *dw = a.val + (size_t)w[q] * a.W;
+        const unsigned long long cd0 = (unsigned long long)d0 + (one0 ? 1u : wt[q]);
+        const unsigned long long cd1 = (unsigned long long)d1 + (one1 ? 1u : wt[q]);
+        const bool i0 = lo && cd0 < c0[q] && cd0 < atomicMin(dw + lane, (uint32_t)cd0);
+        const bool i1 = hi && cd1 < c1[q] && cd1 < atomicMin(dw + 32 + lane, (uint32_t)cd1);
+        const unsigned b0 = __ballot_sync(kFull, i0), b1 = __ballot_sync(kFull, i1);
+        if ((b0 | b1) && lane == 0) {
+          atomicOr(a.front + w[q], (unsigned long long)b0 | ((unsigned long long)b1 << 32));
+          const uint32_t mb = 1u << (w[q] & 31u);
+          uint32_t *bp = a.bm + (w[q] >> 5);
+          if (!(ldcg(bp) & mb)) atomicOr(bp, mb);
+        }
+      }
+    }
+  }
+}
+
+constexpr int kSvSparseMask = 4;
+
 template <int ESZ>
 __device__ __forceinline__ void sv_chunk(const SvArgs &a, const WorkItem &it, unsigned long long f) {
+  if (__popcll(f) > kSvSparseMask) {
+    sv_item_rows<ESZ>(a, it.v, it.eaddr, it.cnt, f);
+    return;
+  }
   constexpr int PER = 16 / ESZ;
   const unsigned lane = lane_id();
   const uintptr_t start = it.eaddr;
@@ -122,6 +186,17 @@ __device__ __forceinline__ void sv_group(const SvArgs &a, unsigned long long fir
   if (idx < n_small) {
     it = a.qs[idx];
     f = a.qsm[idx];
+  }
+  unsigned dense = __ballot_sync(kFull, __popcll(f) > kSvSparseMask);
+  while (dense) {
+    const int i = __ffs(dense) - 1;
+    dense &= dense - 1;
+    sv_item_rows<ESZ>(a, __shfl_sync(kFull, it.v, i), (uintptr_t)shfl64(it.eaddr, i),
+                      __shfl_sync(kFull, it.cnt, i), shfl64(f, i));
+  }
+  if (__popcll(f) > kSvSparseMask) {
+    it.cnt = 0;
+    f = 0;
   }
   const unsigned incl = warp_incl_scan<unsigned>(it.cnt);
   const unsigned excl = incl - it.cnt;
@@ -490,6 +565,9 @@ thv_status step(thv_server *s, uint32_t max_iters, unsigned long long *done, uin
   else
     THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, sv_kernel<4>, kSvThreads, smem));
   if (bpsm < 1) return fail(THV_ECUDA, "serving kernel cannot be resident");
+  // the rotating per-iteration counters restart with every launch
+  const size_t c0 = offsetof(SvCtrl, cnt_small), c1 = offsetof(SvCtrl, thr);
+  THV_CUDA(cudaMemsetAsync((char *)s->d_ctrl + c0, 0, c1 - c0, s->st));
   void *args[] = {&a};
   THV_CUDA(cudaLaunchCooperativeKernel(kern, dim3(bpsm * g->num_sms), dim3(kSvThreads), args, smem, s->st));
   THV_CUDA(cudaMemcpyAsync(s->h_ctrl, s->d_ctrl, sizeof(SvCtrl), cudaMemcpyDeviceToHost, s->st));
