@@ -256,6 +256,27 @@ thv_status thv_serve_stop(thv_server *s);
 thv_status thv_pick_sources(const thv_graph *g, uint64_t seed, uint32_t n,
                             uint32_t *out);
 
+/* ---- allocation-free BFS ---- */
+/* No counterpart in the reference: a BFS for callers that cannot allocate
+ * device memory on this path (a host framework that owns all device memory
+ * through its own pool, or a latency-critical path that cannot take
+ * cudaMalloc's implicit device synchronisation).  Same kernel and results as
+ * thv_run(THV_ALGO_BFS) -- u32 levels, source 1, unreached nv+1 -- over a
+ * CSR the caller already holds in device (or host-mapped) memory: d_off
+ * (nv+1 u64), d_adj (ne u32; 128-byte aligned, readable 16 bytes past its
+ * end, as cudaMalloc allocations are) and the output d_values (nv u32).
+ * It calls no allocator: its scratch is one 64 MiB static device array per
+ * GPU, held until the process exits, so graphs whose scratch needs more
+ * (about 16 bytes per vertex plus 0.3 bytes per edge) get THV_ENOMEM.  Calls
+ * share that array: calls whose work overlaps on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the
+ * array's address; make it before any stream capture.  stream: a
+ * cudaStream_t or NULL; iterations may be NULL.  Synchronous. */
+thv_status thv_bfs_noalloc(const uint64_t *d_off, const uint32_t *d_adj,
+                           uint64_t nv, uint64_t ne, uint32_t source,
+                           uint32_t *d_values, void *stream,
+                           uint64_t *iterations);
+
 /* ---- misc ---- */
 /* Host-link bandwidth of `device` in GB/s: a pinned cudaMemcpy host->device
  * of `bytes`, and a kernel streaming 16-byte zero-copy loads from pinned,

@@ -116,7 +116,7 @@ ABI_FUNCTIONS = [
     "thv_info", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_run",
     "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
-    "thv_pick_sources", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
+    "thv_pick_sources", "thv_bfs_noalloc", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
     "thv_debug_fail_alloc_after",
 ]
 
@@ -147,6 +147,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_get_blocks": ([P, U64, P, P, ctypes.POINTER(ctypes.c_uint64)], I32),
         "thv_link_bandwidth": ([I32, U64, ctypes.POINTER(D), ctypes.POINTER(D)], I32),
         "thv_pick_sources": ([P, U64, U32, P], I32),
+        "thv_bfs_noalloc": ([P, P, U64, U64, U32, P, P, ctypes.POINTER(ctypes.c_uint64)], I32),
         "thv_run": ([P, U32, ctypes.POINTER(_RunOpts), P, ctypes.POINTER(_Stats)], I32),
         "thv_values": ([P, P], I32),
         "thv_write_values": ([ctypes.c_char_p, P, U64, U32], I32),

@@ -35,6 +35,7 @@
 // host link (zero copy).
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 
 #include "thv_device.cuh"
 #include "thv_internal.h"
@@ -643,3 +644,161 @@ const uint32_t *minprop_device_values(thv_graph *g) {
 }
 
 }  // namespace thv
+
+// ============================================== allocation-free BFS entry
+//
+// thv_bfs_noalloc runs the same BFS kernel as thv_run over a CSR that the
+// caller already holds in device (or host-mapped) memory, writing into the
+// caller's value array, and allocates nothing: its scratch (control block,
+// one-entry block table, pending bitmap, work queues) lives in the
+// file-scope array below, which every GPU that loads this library holds
+// until the process exits.  It exists for callers that cannot call
+// cudaMalloc on this path: a host framework that owns all device memory
+// through its own pool or arena, or a latency-critical path that cannot
+// afford cudaMalloc/cudaFree's implicit device synchronisation.
+//
+// All calls share the one array: the kernel reinitialises what must start
+// at zero (bitmap, counters) on every call, and calls whose work overlaps
+// on the GPU (concurrent streams, or several host threads) race on it --
+// serialise them.  The first call on a device looks up the array's device
+// address (cudaGetSymbolAddress); make that first call before any stream
+// capture.
+namespace thv {
+
+constexpr size_t kNoAllocScratchBytes = 64ull << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Host code may not take the array's address directly (a host-side shadow,
+// not a device address): this is the looked-up device address per device.
+static std::mutex g_noalloc_mu;
+static uintptr_t g_noalloc_addr[64];
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct NoAllocLayout {
+  size_t ctrl, table_vb, table_base, bm, qs, qb, total;
+  uint32_t ngroups;
+  uint64_t cap_s, cap_b;
+};
+
+static NoAllocLayout noalloc_layout(uint64_t nv, uint64_t ne) {
+  NoAllocLayout l{};
+  const uint64_t nw = (nv + 31) / 32;
+  l.ngroups = (uint32_t)((nw + 31) / 32);
+  l.cap_s = nv + 32;
+  l.cap_b = ne / kDefaultChunk + ne / kDefaultSmall + 64;
+  size_t off = 0;
+  l.ctrl = off;       off += align256(sizeof(MinCtrl));
+  l.table_vb = off;   off += align256(2 * sizeof(uint32_t));
+  l.table_base = off; off += align256(sizeof(uint64_t));
+  l.bm = off;         off += align256((size_t)l.ngroups * 32 * 4);
+  l.qs = off;         off += align256(l.cap_s * sizeof(MinItem));
+  l.qb = off;         off += align256(l.cap_b * sizeof(MinItem));
+  l.total = off;
+  return l;
+}
+
+// One edge block covering the whole graph, at the caller's adjacency.
+__global__ void noalloc_table_init(uint32_t *vb, uint64_t *base, uint32_t nv, uint64_t adj) {
+  vb[0] = 0;
+  vb[1] = nv;
+  base[0] = adj;
+}
+
+static thv_status noalloc_scratch_address(int dev, uintptr_t *addr) {
+  if (dev < 0 || dev >= 64) return fail(THV_EUNSUPPORTED, "device %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(THV_ECUDA, "cudaGetSymbolAddress(no-alloc scratch): %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = (uintptr_t)p;
+  }
+  *addr = g_noalloc_addr[dev];
+  return THV_OK;
+}
+
+static thv_status bfs_noalloc(const uint64_t *d_off, const uint32_t *d_adj, uint64_t nv,
+                              uint64_t ne, uint32_t source, uint32_t *d_values,
+                              cudaStream_t st, uint64_t *iterations) {
+  if (!d_off || (!d_adj && ne) || !d_values) return fail(THV_EINVAL, "null argument");
+  if (nv == 0 || nv >= 0xFFFFFFFFull) return fail(THV_EINVAL, "vertex count %llu out of range",
+                                                  (unsigned long long)nv);
+  if (source >= nv) return fail(THV_EINVAL, "source %u out of range (n=%llu)", source,
+                                (unsigned long long)nv);
+  if ((uintptr_t)d_adj % 128 != 0)
+    return fail(THV_EINVAL, "adjacency array must be 128-byte aligned");
+  if (((uintptr_t)d_adj + ne * 4) >> 48) return fail(THV_EUNSUPPORTED, "edge address above 2^48");
+  const NoAllocLayout l = noalloc_layout(nv, ne);
+  if (l.total > kNoAllocScratchBytes)
+    return fail(THV_ENOMEM, "graph (n=%llu, m=%llu) needs %zu bytes of scratch; the "
+                "allocation-free entry point holds %zu", (unsigned long long)nv,
+                (unsigned long long)ne, l.total, kNoAllocScratchBytes);
+  int dev = 0;
+  THV_CUDA(cudaGetDevice(&dev));
+  uintptr_t base = 0;
+  THV_TRY(noalloc_scratch_address(dev, &base));
+  cudaDeviceProp prop;
+  THV_CUDA(cudaGetDeviceProperties(&prop, dev));
+
+  MinArgs a{};
+  a.val = d_values;
+  a.bm = (uint32_t *)(base + l.bm);
+  a.wmin = nullptr;  // BFS keeps no pending minima
+  a.off = d_off;
+  a.blk_vb = (const uint32_t *)(base + l.table_vb);
+  a.blk_base = (const uint64_t *)(base + l.table_base);
+  a.host_base = 0;
+  a.qs = (MinItem *)(base + l.qs);
+  a.qb = (MinItem *)(base + l.qb);
+  a.cap_s = l.cap_s;
+  a.cap_b = l.cap_b;
+  a.ctrl = (MinCtrl *)(base + l.ctrl);
+  a.timeout_ns = 60000ull * 1000000ull;
+  a.nblk = 1;
+  a.nv = (uint32_t)nv;
+  a.ngroups = l.ngroups;
+  a.max_iters = (uint32_t)std::min<uint64_t>(nv + 2, 0xFFFFFFF0ull) * 2 + 8;
+  a.delta = 1;
+  a.small_deg = kDefaultSmall;
+  a.chunk = kDefaultChunk;
+  a.src = source;
+  a.growth = kCcGrowth;
+
+  noalloc_table_init<<<1, 1, 0, st>>>((uint32_t *)a.blk_vb, (uint64_t *)a.blk_base, (uint32_t)nv,
+                                      (uint64_t)(uintptr_t)d_adj);
+  const int init_grid = std::max(1, std::min<int>(prop.multiProcessorCount * 8, (int)((nv + 255) / 256)));
+  minprop_init<OP_BFS><<<init_grid, 256, 0, st>>>(a, l.ngroups * 32u);
+  THV_CUDA(cudaGetLastError());
+  auto kern = minprop_kernel<OP_BFS, 4>;
+  const size_t smem = 1 * 8 + 2 * 4;
+  int bpsm = 0;
+  THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kMinThreads, smem));
+  if (bpsm < 1) return fail(THV_ECUDA, "BFS kernel cannot be resident");
+  void *args[] = {&a};
+  THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(bpsm * prop.multiProcessorCount),
+                                       dim3(kMinThreads), args, smem, st));
+  MinCtrl hc;  // the caller's stack: nothing allocated
+  THV_CUDA(cudaMemcpyAsync(&hc, a.ctrl, sizeof(MinCtrl), cudaMemcpyDeviceToHost, st));
+  THV_CUDA(cudaStreamSynchronize(st));
+  if (iterations) *iterations = hc.iters;
+  if (hc.err == kDevErrBarrier) return fail(THV_ETIMEOUT, "grid barrier wait timed out");
+  if (hc.err == kDevErrIters) return fail(THV_ETIMEOUT, "iteration cap reached");
+  if (hc.err == kDevErrQueue) return fail(THV_EDEVICE, "work queue overflow");
+  if (hc.err) return fail(THV_EDEVICE, "device error %u", hc.err);
+  return THV_OK;
+}
+
+}  // namespace thv
+
+extern "C" thv_status thv_bfs_noalloc(const uint64_t *d_off, const uint32_t *d_adj, uint64_t nv,
+                                      uint64_t ne, uint32_t source, uint32_t *d_values,
+                                      void *stream, uint64_t *iterations) {
+  try {
+    return thv::bfs_noalloc(d_off, d_adj, nv, ne, source, d_values, (cudaStream_t)stream,
+                            iterations);
+  } catch (...) {
+    return thv::fail(THV_EINVAL, "exception in thv_bfs_noalloc");
+  }
+}
