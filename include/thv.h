@@ -145,7 +145,8 @@ typedef struct thv_run_opts {
   uint32_t source;       /* BFS / SSSP */
   uint32_t pr_iters;     /* 0 = 20 */
   double pr_damping;     /* 0 = 0.85 */
-  uint32_t sssp_delta;   /* near/far split width; 0 = auto */
+  uint32_t sssp_delta;   /* SSSP near/far window (0 = 8); CC initial label
+                            window (0 = 1) */
   uint32_t timeout_ms;   /* bound on any device-side wait; 0 = 60000 */
   void *stream;          /* cudaStream_t to launch on; NULL = graph's own */
   uint32_t small_degree; /* expansion tuning; 0 = default */
@@ -157,6 +158,13 @@ typedef struct thv_run_opts {
 /* thv_run_opts.flags: also compute stats->checksum = sum over v of
  * splitmix64((v << 32) | value) (BFS/CC/SSSP), after the timed traversal */
 #define THV_RUN_CHECKSUM 1u
+/* BFS/CC/SSSP work-queue construction; same results either way.  Scan:
+ * rebuild the queue from the pending bitmap every iteration (sorted vertex
+ * order, two grid barriers per iteration; the default for BFS and CC).
+ * Queue: queue vertices as they are lowered, scanning only when the near
+ * window empties (one barrier per iteration; the default for SSSP). */
+#define THV_RUN_SCAN_COMPACTION 2u
+#define THV_RUN_QUEUE_COMPACTION 4u
 
 typedef struct thv_stats {
   double device_ms;         /* CUDA-event time of the traversal */

@@ -278,3 +278,20 @@ def test_run_checksum_flag(T, O, g14):
         plan(g, 0.4)
         vals, st = g.run("bfs", source=1, checksum=True)
         assert st["checksum"] == T.values_checksum(vals)
+
+
+@pytest.mark.parametrize("frac", [0.0, 0.4])
+def test_scan_and_queue_compaction_agree(T, O, g14w, frac):
+    """Both work-queue constructions (bitmap scan every iteration, or
+    queueing vertices as they are lowered) give the oracle's values."""
+    with engine_graph(T, g14w, "wcsr") as g:
+        plan(g, frac)
+        for src in O.sources(g14w, 2).tolist():
+            for mode in ("scan", "queue"):
+                got, _ = g.run("bfs", source=src, compaction=mode, timeout_ms=20000)
+                assert np.array_equal(got, O.bfs(g14w, src))
+                got, _ = g.run("sssp", source=src, compaction=mode, timeout_ms=20000)
+                assert np.array_equal(got, O.sssp(g14w, src))
+        for mode in ("scan", "queue"):
+            got, _ = g.run("cc", compaction=mode, timeout_ms=20000)
+            assert np.array_equal(got, O.cc(g14w))

@@ -261,12 +261,15 @@ class Graph:
     def run(self, algo: str, source: int = 1, pr_iters: int = 20, pr_damping: float = 0.85,
             out: Optional[np.ndarray] = None, want_values: bool = True, stream: int = 0,
             sssp_delta: int = 0, timeout_ms: int = 0, small_degree: int = 0,
-            chunk_edges: int = 0, checksum: bool = False):
-        """Run algo; returns (values or None, stats dict)."""
+            chunk_edges: int = 0, checksum: bool = False, compaction: str = ""):
+        """Run algo; returns (values or None, stats dict).  compaction:
+        "" (per-algorithm default), "scan" or "queue"."""
         lib = load_library()
+        flags = ((1 if checksum else 0) | (2 if compaction == "scan" else 0)
+                 | (4 if compaction == "queue" else 0))
         o = _RunOpts(source, pr_iters, pr_damping, sssp_delta, timeout_ms,
                      ctypes.c_void_p(stream) if stream else None, small_degree, chunk_edges,
-                     1 if checksum else 0, 0)
+                     flags, 0)
         st = _Stats()
         buf = None
         if want_values:

@@ -47,7 +47,10 @@ enum { OP_BFS = 0, OP_CC = 1, OP_SSSP = 2 };
 constexpr int kMinThreads = 512;
 constexpr uint32_t kDefaultSmall = 64;  // degree < this: warp-cooperative
 constexpr uint32_t kDefaultChunk = 256; // edges per high-degree work item
-constexpr uint32_t kDefaultDelta = 2;   // SSSP near/far width (weights >= 1)
+// SSSP near/far width.  Measured at RMAT-24 (40% in HBM): width 2 expands
+// every vertex once (link bytes = algorithmic) but needs ~200 iterations;
+// width 8 re-reads 5% more adjacency in ~80 iterations and is fastest.
+constexpr uint32_t kDefaultDelta = 8;
 constexpr uint32_t kCcGrowth = 8;       // CC label window growth per advance
 
 
@@ -86,6 +89,9 @@ struct MinArgs {
   MinItem *qs, *qb;
   unsigned long long cap_s, cap_b;
   MinCtrl *ctrl;
+  // queue mode: second queue buffers and the "queued" bitmap
+  MinItem *qs2, *qb2;
+  uint32_t *qd;
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, max_iters;
   uint32_t delta, small_deg, chunk, src;
@@ -98,6 +104,8 @@ struct MinState {
   uint32_t *d_bm = nullptr;
   uint32_t *d_wmin = nullptr;
   MinItem *d_qs = nullptr, *d_qb = nullptr;
+  MinItem *d_qs2 = nullptr, *d_qb2 = nullptr;
+  uint32_t *d_qd = nullptr;
   uint64_t cap_s = 0, cap_b = 0;
   uint32_t chunk = 0, small = 0;
   MinCtrl *d_ctrl = nullptr;
@@ -441,6 +449,358 @@ __global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
   }
 }
 
+// ================================================================ queue mode
+//
+// Same relaxation and windows as minprop_kernel, but a relaxation that
+// lowers a vertex below the window pushes it straight into the next
+// iteration's queue (degree, block and warp-aggregated append done by the
+// pusher), so an iteration is one expansion phase and one grid barrier.
+// The bitmap scan runs only when the near queue is empty: at the start, and
+// when an SSSP/CC window advances over vertices parked in the far bitmap.
+//
+// SSSP/CC push once per queue through a "queued" bit.  Ordering: the pusher
+// does atomicMin(val); fence.sc; atomicOr(queued) and pushes only if the bit
+// was clear; the expander does atomicAnd(queued, ~bit); fence.sc; load val.
+// With sequentially consistent fences on both sides at least one of them
+// sees the other: either the expansion reads the lowered value, or the
+// pusher sees the bit cleared and queues the vertex again -- no decrease is
+// lost.  BFS needs neither: a vertex changes once, its pusher is unique.
+
+__device__ __forceinline__ void fence_sc() { asm volatile("fence.sc.gpu;" ::: "memory"); }
+
+struct QStats {
+  unsigned long long edges = 0, hbm = 0, link = 0, verts = 0;
+};
+
+// Warp-uniform: lanes with `flag` append vertex w (value wval) to the queue
+// pair (qs, qb) whose counters live in slot cs.
+template <int ESZ>
+__device__ __forceinline__ void q_append(const MinArgs &a, const uint32_t *vb,
+                                         const unsigned long long *bbase, MinItem *qs,
+                                         MinItem *qb, unsigned cs, bool flag, uint32_t w,
+                                         uint32_t wval, QStats &qst) {
+  if (!__any_sync(kFull, flag)) return;
+  MinCtrl *c = a.ctrl;
+  const unsigned lane = lane_id();
+  uint32_t deg = 0;
+  unsigned long long eaddr = 0;
+  if (flag) {
+    const uint64_t s0 = __ldg(a.off + w), e0 = __ldg(a.off + w + 1);
+    deg = (uint32_t)(e0 - s0);
+    const unsigned long long base = bbase[find_block(vb, a.nblk, w)];
+    eaddr = base + s0 * ESZ;
+    qst.edges += deg;
+    qst.verts += 1;
+    if (base == a.host_base) qst.link += (unsigned long long)deg * ESZ;
+    else qst.hbm += (unsigned long long)deg * ESZ;
+  }
+  const bool small = flag && deg > 0 && deg < a.small_deg;
+  const bool big = flag && deg >= a.small_deg;
+  const unsigned sm = __ballot_sync(kFull, small);
+  if (sm) {
+    const int ldr = __ffs(sm) - 1;
+    unsigned long long base = 0;
+    if (lane == (unsigned)ldr) base = atomicAdd(&c->cnt_small[cs], (unsigned long long)__popc(sm));
+    base = shfl64(base, ldr);
+    const unsigned long long pos = base + __popc(sm & lanemask_lt());
+    if (small) {
+      if (pos < a.cap_s) qs[pos] = make_item(eaddr, deg, w, wval);
+      else atomicCAS(&c->err, 0u, kDevErrQueue);
+    }
+  }
+  if (__any_sync(kFull, big)) {
+    const unsigned nch = big ? (deg + a.chunk - 1) / a.chunk : 0u;
+    const unsigned inc = warp_incl_scan<unsigned>(nch);
+    const unsigned tot = __shfl_sync(kFull, inc, 31);
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(&c->cnt_big[cs], (unsigned long long)tot);
+    base = shfl64(base, 0);
+    if (big) {
+      unsigned long long pos = base + inc - nch;
+      for (unsigned k = 0; k < nch; k++, pos++) {
+        const uint32_t lo = k * a.chunk;
+        if (pos < a.cap_b)
+          qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, min(a.chunk, deg - lo), w, wval);
+        else
+          atomicCAS(&c->err, 0u, kDevErrQueue);
+      }
+    }
+  }
+}
+
+struct QEnv {
+  const uint32_t *vb;
+  const unsigned long long *bbase;
+  MinItem *qs_next, *qb_next;
+  unsigned cs_next;
+  uint32_t thr;
+};
+
+// Relax N edges per lane; near improvements are queued, far ones parked.
+template <int OP, int ESZ, int N>
+__device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const uint32_t (&w)[N],
+                                          const unsigned long long (&cand)[N], const bool (&ok)[N],
+                                          QStats &qst) {
+  uint32_t cur[N];
+  bool push[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) cur[j] = ok[j] ? ldcg(a.val + w[j]) : 0u;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    push[j] = false;
+    if (ok[j] && cand[j] < cur[j]) {
+      const uint32_t old = atomicMin(a.val + w[j], (uint32_t)cand[j]);
+      if (cand[j] < old) {
+        if (OP == OP_BFS) {
+          push[j] = true;
+        } else if (cand[j] < e.thr) {
+          fence_sc();
+          const uint32_t m = 1u << (w[j] & 31u);
+          push[j] = !(atomicOr(a.qd + (w[j] >> 5), m) & m);
+        } else {
+          atomicMin(a.wmin + (w[j] >> 5), (uint32_t)cand[j]);
+          const uint32_t m = 1u << (w[j] & 31u);
+          uint32_t *bp = a.bm + (w[j] >> 5);
+          if (!(ldcg(bp) & m)) atomicOr(bp, m);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < N; j++)
+    q_append<ESZ>(a, e.vb, e.bbase, e.qs_next, e.qb_next, e.cs_next, push[j], w[j],
+                  (uint32_t)cand[j], qst);
+}
+
+// Value of a dequeued vertex: BFS values are final when queued; SSSP/CC
+// clear the vertex's queued and parked bits, fence, then read the latest.
+template <int OP>
+__device__ __forceinline__ uint32_t q_dequeue(const MinArgs &a, bool valid, uint32_t v,
+                                              uint32_t item_val) {
+  if (OP == OP_BFS) return item_val;
+  const uint32_t m = 1u << (v & 31u);
+  if (valid) {
+    atomicAnd(a.qd + (v >> 5), ~m);
+    if (ldcg(a.bm + (v >> 5)) & m) atomicAnd(a.bm + (v >> 5), ~m);
+  }
+  fence_sc();
+  return valid ? ldcg(a.val + v) : 0u;
+}
+
+template <int OP, int ESZ>
+__device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const MinItem &it,
+                                        QStats &qst) {
+  constexpr int PER = 16 / ESZ;
+  const unsigned lane = lane_id();
+  uint32_t vval = 0;
+  if (OP == OP_BFS) vval = it.val;
+  else vval = __shfl_sync(kFull, q_dequeue<OP>(a, lane == 0, it.v, it.val), 0);
+  const uintptr_t start = it.ea_cnt & kAddrMask;
+  const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
+  for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; __any_sync(kFull, p < end); p += 512u) {
+    const bool in = p < end;
+    const uint4 q = in ? ld_nc_v4(p) : make_uint4(0, 0, 0, 0);
+    const uint32_t f[4] = {q.x, q.y, q.z, q.w};
+    uint32_t w[PER];
+    unsigned long long cand[PER];
+    bool ok[PER];
+#pragma unroll
+    for (int j = 0; j < PER; j++) {
+      const uintptr_t ea = p + (uintptr_t)ESZ * j;
+      ok[j] = in && ea >= start && ea < end;
+      w[j] = ESZ == 4 ? f[j] : f[2 * j];
+      cand[j] = candidate<OP>(vval, ESZ == 4 ? 0u : f[2 * j + 1]);
+    }
+    q_relax_n<OP, ESZ, PER>(a, e, w, cand, ok, qst);
+  }
+}
+
+template <int OP, int ESZ>
+__device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const MinItem *qs,
+                                        unsigned long long first, unsigned long long n_small,
+                                        QStats &qst) {
+  const unsigned lane = lane_id();
+  const unsigned long long idx = first + lane;
+  MinItem it{0, 0, 0};
+  const bool valid = idx < n_small;
+  if (valid) it = qs[idx];
+  const uint32_t vval = q_dequeue<OP>(a, valid, it.v, it.val);
+  const unsigned cnt = (unsigned)(it.ea_cnt >> 48);
+  const unsigned long long eaddr = it.ea_cnt & kAddrMask;
+  const unsigned incl = warp_incl_scan<unsigned>(cnt);
+  const unsigned excl = incl - cnt;
+  const unsigned total = __shfl_sync(kFull, incl, 31);
+  for (unsigned k = 0; k < total; k += 32) {
+    const unsigned t = k + lane;
+    const int o = warp_owner(excl, t);
+    const unsigned long long ea = shfl64(eaddr, o);
+    const unsigned oex = __shfl_sync(kFull, excl, o);
+    const uint32_t ov = __shfl_sync(kFull, vval, o);
+    uint32_t w[1] = {0};
+    unsigned long long cand[1];
+    bool ok[1] = {t < total};
+    uint32_t wt = 0;
+    if (ok[0]) {
+      const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
+      if (ESZ == 4) {
+        w[0] = ld_nc_u32(addr);
+      } else {
+        const uint2 ed = ld_nc_u2(addr);
+        w[0] = ed.x;
+        wt = ed.y;
+      }
+    }
+    cand[0] = candidate<OP>(ov, wt);
+    q_relax_n<OP, ESZ, 1>(a, e, w, cand, ok, qst);
+  }
+}
+
+template <int OP, int ESZ>
+__global__ void __launch_bounds__(kMinThreads) minq_kernel(MinArgs a) {
+  extern __shared__ unsigned long long s_tab[];
+  const bool smem_tab = a.nblk <= kSmemBlocks;
+  unsigned long long *s_base = s_tab;
+  uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_tab + a.nblk);
+  if (smem_tab) {
+    for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x) s_vb[i] = a.blk_vb[i];
+    for (uint32_t i = threadIdx.x; i < a.nblk; i += blockDim.x) s_base[i] = a.blk_base[i];
+  }
+  __syncthreads();
+  QEnv env;
+  env.vb = smem_tab ? s_vb : a.blk_vb;
+  env.bbase = smem_tab ? s_base : (const unsigned long long *)a.blk_base;
+  MinCtrl *c = a.ctrl;
+  const unsigned lane = lane_id();
+  const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  uint32_t thr = 0xFFFFFFFFu;
+  uint32_t width = a.delta;
+  if (OP == OP_SSSP) thr = (uint32_t)min(1ull + a.delta, 0xFFFFFFFFull);
+  if (OP == OP_CC) thr = a.delta;
+  QStats qst;
+  // Every phase (scan or expansion) ph produces the queue in counter slot
+  // ph % 3 and buffer ph & 1; an expansion consumes what phase ph - 1
+  // produced.  The decision after a phase reads only that phase's slot,
+  // which no block writes again before everyone has passed the next
+  // barrier; the leader clears slot (ph + 1) % 3 at the start of phase ph.
+  unsigned ph = 0, iter = 0;
+  bool scan = true;
+  for (;; ++iter, ++ph) {
+    if (iter >= a.max_iters) {
+      if (leader) atomicCAS(&c->err, 0u, kDevErrIters);
+      break;
+    }
+    const unsigned cur = ph % 3, prev = (ph + 2) % 3;
+    if (leader) {
+      const unsigned r = (ph + 1) % 3;
+      c->cnt_small[r] = 0;
+      c->cnt_big[r] = 0;
+      c->wc[r] = 0;
+      c->remaining[r] = 0;
+      c->minkept[r] = 0xFFFFFFFFu;
+    }
+    MinItem *qs_out = (ph & 1) ? a.qs2 : a.qs, *qb_out = (ph & 1) ? a.qb2 : a.qb;
+    MinItem *qs_in = (ph & 1) ? a.qs : a.qs2, *qb_in = (ph & 1) ? a.qb : a.qb2;
+    env.qs_next = qs_out;
+    env.qb_next = qb_out;
+    env.cs_next = cur;
+    env.thr = thr;
+    if (scan) {
+      // ------------------------------------------------------------- scan
+      unsigned long long my_keep = 0;
+      uint32_t my_min = 0xFFFFFFFFu;
+      for (unsigned g = gwarp; g < a.ngroups; g += nwarps) {
+        const unsigned wbase = g * 32u;
+        const uint32_t word = ldcg(a.bm + wbase + lane);
+        unsigned nz = __ballot_sync(kFull, word != 0);
+        if (OP != OP_BFS) {
+          const uint32_t wm = word ? ldcg(a.wmin + wbase + lane) : 0xFFFFFFFFu;
+          if (word != 0 && wm >= thr) {
+            my_keep += __popc(word);
+            my_min = min(my_min, wm);
+          }
+          nz = __ballot_sync(kFull, word != 0 && wm < thr);
+        }
+        while (nz) {
+          const int j = __ffs(nz) - 1;
+          nz &= nz - 1;
+          const uint32_t wd = __shfl_sync(kFull, word, j);
+          const uint32_t v = (wbase + j) * 32u + lane;
+          const bool act = (wd >> lane) & 1u;
+          const uint32_t vval = act ? ldcg(a.val + v) : 0u;
+          const bool take = act && (OP == OP_BFS || vval < thr);
+          const unsigned tm = __ballot_sync(kFull, take);
+          if (OP != OP_BFS) {
+            const uint32_t kmin = warp_min(act && !take ? vval : 0xFFFFFFFFu);
+            my_min = min(my_min, kmin);
+            if (lane == 0) {
+              my_keep += __popc(wd & ~tm);
+              a.wmin[wbase + j] = kmin;
+              if (tm) atomicOr(a.qd + wbase + j, tm);
+            }
+          }
+          if (lane == 0 && tm) a.bm[wbase + j] = wd & ~tm;
+          q_append<ESZ>(a, env.vb, env.bbase, qs_out, qb_out, cur, take, v, vval, qst);
+        }
+      }
+      if (OP != OP_BFS) {
+        my_keep = warp_sum(my_keep);
+        my_min = warp_min(my_min);
+        if (lane == 0) {
+          if (my_keep) atomicAdd(&c->remaining[cur], my_keep);
+          if (my_min != 0xFFFFFFFFu) atomicMin(&c->minkept[cur], my_min);
+        }
+      }
+    } else {
+      // --------------------------------------------------------- expansion
+      const unsigned long long ns = ldcg(&c->cnt_small[prev]);
+      const unsigned long long nb = ldcg(&c->cnt_big[prev]);
+      const unsigned long long ntask = nb + (ns + 31) / 32;
+      for (unsigned long long t = gwarp; t < ntask;) {
+        unsigned long long nt = 0;
+        if (lane == 0) nt = atomicAdd(&c->wc[prev], 1ull);
+        if (t < nb) {
+          const MinItem it = qb_in[t];
+          q_chunk<OP, ESZ>(a, env, it, qst);
+        } else {
+          q_group<OP, ESZ>(a, env, qs_in, (t - nb) * 32ull, ns, qst);
+        }
+        t = nwarps + shfl64(nt, 0);
+      }
+    }
+    if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+    const unsigned long long produced = ldcg(&c->cnt_small[cur]) + ldcg(&c->cnt_big[cur]);
+    if (produced) {
+      scan = false;  // expand what this phase queued
+    } else if (!scan) {
+      scan = true;   // near queue empty: look at the parked vertices
+    } else {
+      if (OP == OP_BFS || ldcg(&c->remaining[cur]) == 0) break;
+      const uint32_t mk = ldcg(&c->minkept[cur]);
+      if (OP == OP_CC) width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
+      thr = (uint32_t)min((unsigned long long)mk + width, 0xFFFFFFFFull);
+    }
+  }
+  qst.edges = warp_sum(qst.edges);
+  qst.hbm = warp_sum(qst.hbm);
+  qst.link = warp_sum(qst.link);
+  qst.verts = warp_sum(qst.verts);
+  if (lane == 0 && qst.verts) {
+    atomicAdd(&c->edges, qst.edges);
+    atomicAdd(&c->hbm_bytes, qst.hbm);
+    atomicAdd(&c->link_bytes, qst.link);
+    atomicAdd(&c->vertices, qst.verts);
+  }
+  if (leader) c->iters = iter;
+}
+
+template <int OP>
+__global__ void minq_clear(uint32_t *qd, uint32_t nw_alloc) {
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nw_alloc; w += gridDim.x * blockDim.x)
+    qd[w] = 0;
+}
+
 __global__ void values_checksum_kernel(const uint32_t *val, uint64_t nv,
                                        unsigned long long *sum) {
   __shared__ unsigned long long s_red[32];
@@ -485,6 +845,9 @@ static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
   THV_TRY(dev_alloc((void **)&ms->d_wmin, nw_alloc * 4, "pending minima"));
   THV_TRY(dev_alloc((void **)&ms->d_qs, ms->cap_s * sizeof(MinItem), "queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(MinItem), "chunk queue"));
+  THV_TRY(dev_alloc((void **)&ms->d_qs2, ms->cap_s * sizeof(MinItem), "queue"));
+  THV_TRY(dev_alloc((void **)&ms->d_qb2, ms->cap_b * sizeof(MinItem), "chunk queue"));
+  THV_TRY(dev_alloc((void **)&ms->d_qd, nw_alloc * 4, "queued bitmap"));
   THV_TRY(dev_alloc((void **)&ms->d_ctrl, sizeof(MinCtrl), "control"));
   THV_TRY(pinned_alloc((void **)&ms->h_ctrl, sizeof(MinCtrl), "control"));
   THV_CUDA(cudaEventCreate(&ms->ev0));
@@ -501,6 +864,9 @@ void minprop_free(thv_graph *g) {
   dev_free(ms->d_wmin);
   dev_free(ms->d_qs);
   dev_free(ms->d_qb);
+  dev_free(ms->d_qs2);
+  dev_free(ms->d_qb2);
+  dev_free(ms->d_qd);
   dev_free(ms->d_ctrl);
   pinned_free(ms->h_ctrl);
   if (ms->ev0) cudaEventDestroy(ms->ev0);
@@ -511,8 +877,8 @@ void minprop_free(thv_graph *g) {
 
 template <int OP, int ESZ>
 static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
-                                 uint32_t &launches) {
-  auto kern = minprop_kernel<OP, ESZ>;
+                                 uint32_t &launches, bool scan_mode) {
+  auto kern = scan_mode ? minprop_kernel<OP, ESZ> : minq_kernel<OP, ESZ>;
   const size_t nb = g->plan.blocks.size();
   const size_t smem = nb <= kSmemBlocks ? nb * 8 + (nb + 1) * 4 : 0;
   int bpsm = 0;
@@ -524,6 +890,10 @@ static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
   const int init_grid = std::max(1, std::min<int>(g->num_sms * 8,
                                 (int)((g->nv + 255) / 256)));
   minprop_init<OP><<<init_grid, 256, 0, st>>>(a, nw_alloc);
+  if (!scan_mode) {
+    minq_clear<OP><<<init_grid, 256, 0, st>>>(a.qd, nw_alloc);
+    launches++;
+  }
   THV_CUDA(cudaGetLastError());
   void *args[] = {&a};
   THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(grid),
@@ -569,6 +939,9 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.host_base = g->h_edges_dev;
   a.qs = ms->d_qs;
   a.qb = ms->d_qb;
+  a.qs2 = ms->d_qs2;
+  a.qb2 = ms->d_qb2;
+  a.qd = ms->d_qd;
   a.cap_s = ms->cap_s;
   a.cap_b = ms->cap_b;
   a.ctrl = ms->d_ctrl;
@@ -587,14 +960,19 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   uint32_t launches = 0;
   THV_CUDA(cudaEventRecord(ms->ev0, st));
   thv_status s = THV_OK;
+  // scan-built queues keep vertex order (coalesced offset reads) and no
+  // fences: better for BFS and CC; SSSP gains from fewer barriers
+  bool scan_mode = op != OP_SSSP;
+  if (o && (o->flags & THV_RUN_SCAN_COMPACTION)) scan_mode = true;
+  if (o && (o->flags & THV_RUN_QUEUE_COMPACTION)) scan_mode = false;
   if (g->esz == 4) {
-    if (op == OP_BFS) s = launch_minprop<OP_BFS, 4>(g, a, st, launches);
-    else if (op == OP_CC) s = launch_minprop<OP_CC, 4>(g, a, st, launches);
+    if (op == OP_BFS) s = launch_minprop<OP_BFS, 4>(g, a, st, launches, scan_mode);
+    else if (op == OP_CC) s = launch_minprop<OP_CC, 4>(g, a, st, launches, scan_mode);
     else s = fail(THV_EINVAL, "SSSP needs 8-byte weighted edges");
   } else {
-    if (op == OP_BFS) s = launch_minprop<OP_BFS, 8>(g, a, st, launches);
-    else if (op == OP_CC) s = launch_minprop<OP_CC, 8>(g, a, st, launches);
-    else s = launch_minprop<OP_SSSP, 8>(g, a, st, launches);
+    if (op == OP_BFS) s = launch_minprop<OP_BFS, 8>(g, a, st, launches, scan_mode);
+    else if (op == OP_CC) s = launch_minprop<OP_CC, 8>(g, a, st, launches, scan_mode);
+    else s = launch_minprop<OP_SSSP, 8>(g, a, st, launches, scan_mode);
   }
   if (s != THV_OK) return s;
   THV_CUDA(cudaEventRecord(ms->ev1, st));
