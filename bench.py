@@ -72,7 +72,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2cc", "c3", "c4", "c5"])
     ap.add_argument("--edge-factor", type=int, default=0, help="override the edge factor")
     ap.add_argument("--rates", default="", help="c5: comma-separated arrival rates (queries/s)")
     ap.add_argument("--sssp-delta", type=int, default=0, help="c4: batched SSSP window width")
@@ -179,12 +179,14 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def algorithmic_bytes(off, vals, nv, vb, res, esz, algo, n_iters=1):
+def algorithmic_bytes(off, vals, nv, vb, res, esz, algo, n_iters=1, list_deg=0):
     """Per-run bytes a work-optimal run must move, split HBM / host link.
 
     BFS/SSSP: every reached vertex is expanded once: 16 B of offsets and a
-    4 B value write, its adjacency (esz per edge; over the host link when its
-    block is not resident) and a 4 B value probe per edge.  CC/PR: every
+    4 B value write, its adjacency (esz per edge as stored: 4 B for packed
+    weighted edges; over the host link when its
+    block is not resident and the list is not in the small-list cache,
+    0 < deg < list_deg) and a 4 B value probe per edge.  CC/PR: every
     vertex once per iteration (CC: the synchronous label-propagation sweep
     count is not fixed, so the bytes of ONE full sweep are used -- a lower
     bound)."""
@@ -194,7 +196,7 @@ def algorithmic_bytes(off, vals, nv, vb, res, esz, algo, n_iters=1):
     else:
         mask = np.ones(nv, bool)
     blk = np.searchsorted(vb.astype(np.int64), np.arange(nv), side="right") - 1
-    resident_v = res[blk]
+    resident_v = res[blk] | ((deg > 0) & (deg < list_deg))
     d = deg[mask]
     r = resident_v[mask]
     per_edge_probe = 4 if algo != "pr_push" else 8
@@ -228,8 +230,9 @@ def run_ours(args, dist):
         g = T.Graph.generate_rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"],
                                   fmt=wl["fmt"], device=dev)
         budget = wl.get("budget", int(wl.get("frac", 1.0) * g.ne * g.esz))
-        plan = g.plan(budget)
         algo = wl["algo"]
+        # PageRank reads whole blocks: no small-list cache
+        plan = g.plan(budget, small_list_degree=1 if algo.startswith("pr") else 0)
         src = args.source
         sptr = stream.cuda_stream
         for _ in range(w):
@@ -238,8 +241,9 @@ def run_ours(args, dist):
         off, edges, _ = g.host_arrays()
         vb, res = g.blocks()
         iters = 20 if algo.startswith("pr") else 1
+        lcd = 0 if algo.startswith("pr") else plan["small_list_degree"]
         b_hbm, b_link, trav = algorithmic_bytes(off, vals if algo in ("bfs", "sssp") else None,
-                                                g.nv, vb, res, g.esz, algo, iters)
+                                                g.nv, vb, res, g.mem_esz, algo, iters, lcd)
         if algo == "cc" or algo.startswith("pr"):
             trav = g.ne * iters
         clocks = Clocks(dev)
@@ -271,6 +275,8 @@ def run_ours(args, dist):
         out = {
             "value": value, "ms_per_step": total_s * 1e3 / k, "traversed_edges": trav,
             "plan": plan, "clocks": ck, "gpu_launches": launches,
+            "storage": {"format_edge_bytes": g.esz, "stored_edge_bytes": g.mem_esz,
+                        "packed_weight_bits": g.weight_bits, "budget_bytes": budget},
             "roofline": {
                 "bound": "hbm", "unit": "GB/s",
                 "achieved": (b_hbm + b_link) / kern_s / 1e9,
@@ -492,7 +498,9 @@ def main():
                     "config": {"workload": f"c5 serving rmat{scale} ef{ef} wcsr, {int(frac * 100)}% of "
                                            f"edge bytes in HBM, {args.queries} queries per rate",
                                "resident_edge_bytes": plan["resident_edge_bytes"],
-                               "host_edge_bytes": plan["host_edge_bytes"]},
+                               "host_edge_bytes": plan["host_edge_bytes"],
+                               "small_list_cache": {k: plan[k] for k in (
+                                   "small_list_degree", "small_list_bytes", "small_list_vertices")}},
                     "plain_mean_ms": plain_mean, "sweep": sweep}
             print(json.dumps(line))
         dist.close()
@@ -514,7 +522,8 @@ def main():
         return
     wl, m, extra = run_ours(args, dist)
     if dist.rank == 0:
-        budget_desc = (f"{int(wl['frac'] * 100)}% of edge bytes" if "frac" in wl else f"{wl['budget']} bytes")
+        budget_desc = (f"{int(wl['frac'] * 100)}% of the format's edge bytes" if "frac" in wl
+                       else f"{wl['budget']} bytes")
         line = {
             "metric": f"GTEPS ({wl['algo']})", "value": m["value"], "unit": "GTEPS",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -527,6 +536,9 @@ def main():
                        "hbm_edge_budget": budget_desc, "source": args.source,
                        "resident_edge_bytes": m["plan"]["resident_edge_bytes"],
                        "host_edge_bytes": m["plan"]["host_edge_bytes"],
+                       "small_list_cache": {k: m["plan"][k] for k in (
+                           "small_list_degree", "small_list_bytes", "small_list_vertices")},
+                       "edge_storage": m["storage"],
                        "traversed_edges_per_step": m["traversed_edges"],
                        "parallelism": f"replicas x{args.gpus}",
                        "l2": "256 MiB device write between timed steps (outside the events)"},

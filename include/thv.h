@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define THV_ABI_VERSION 1
+#define THV_ABI_VERSION 2
 
 typedef enum thv_status {
   THV_OK = 0,
@@ -107,11 +107,21 @@ thv_status thv_close(thv_graph *g);
 
 typedef struct thv_graph_info {
   uint64_t nv, ne;
-  uint32_t fmt, esz;    /* in-memory edge size: 4 or 8 */
+  uint32_t fmt, esz;    /* edge size of the format: 8 for weighted, else 4 */
   uint32_t device, weighted;
+  uint32_t mem_esz;     /* bytes per edge as stored (host and HBM): 4 when packed */
+  uint32_t weight_bits; /* packed: low bits of an edge hold w - min weight; 0 = not packed */
 } thv_graph_info;
 thv_status thv_info(const thv_graph *g, thv_graph_info *out);
-/* Host views of the graph (valid until thv_close). outdeg NULL unless CSC. */
+/* Weighted graphs are stored packed by default: each {u32 dst, u32 w} pair
+ * becomes one u32, dst << b | (w - min w), whenever the id bits plus the
+ * weight-range bits fit 32 bits (lossless; halves the edge bytes moved).
+ * packed = 0 restores {dst, w} pairs, 1 packs again.  Drops the plan;
+ * no effect on unweighted graphs. */
+thv_status thv_set_edge_packing(thv_graph *g, int packed);
+/* Host views of the graph (valid until thv_close); edges in the format's
+ * layout ({dst, w} pairs for weighted graphs, unpacked on first use).
+ * outdeg NULL unless CSC. */
 thv_status thv_host_arrays(const thv_graph *g, const uint64_t **off,
                            const void **edges, const uint32_t **outdeg);
 
@@ -123,13 +133,22 @@ typedef struct thv_plan_opts {
   uint64_t hbm_budget_bytes; /* resident edge bytes; UINT64_MAX = all that fit */
   uint64_t block_bytes;      /* edge block size; 0 = 64 MiB */
   uint32_t policy;
-  uint32_t pad;
+  /* Small-list cache: adjacency lists with 0 < degree < small_list_degree
+   * that fall in host blocks are copied, packed, into HBM first (host reads
+   * of short lists are bound by the link's request rate, not its bytes);
+   * blocks fill the rest of the budget.  The threshold is lowered until
+   * the lists fit the budget.  BFS/CC/SSSP and the batched and served runs
+   * read the cache; PageRank reads whole blocks and ignores it.
+   * 0 = default (64 for CSR/WCSR, off for CSC); 1 = off. */
+  uint32_t small_list_degree;
 } thv_plan_opts;
 
 typedef struct thv_plan_info {
   uint64_t num_blocks, resident_blocks;
-  uint64_t resident_edge_bytes, host_edge_bytes;
+  uint64_t resident_edge_bytes, host_edge_bytes; /* resident includes the cache */
   uint64_t device_bytes; /* all device memory the graph holds */
+  uint64_t small_list_degree; /* effective threshold; 0 = no cache */
+  uint64_t small_list_bytes, small_list_vertices;
 } thv_plan_info;
 
 thv_status thv_plan(thv_graph *g, const thv_plan_opts *o); /* NULL = defaults */

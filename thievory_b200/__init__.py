@@ -66,19 +66,21 @@ class _Stats(ctypes.Structure):
 
 class _PlanOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("block_bytes", ctypes.c_uint64),
-                ("policy", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+                ("policy", ctypes.c_uint32), ("small_list_degree", ctypes.c_uint32)]
 
 
 class _PlanInfo(ctypes.Structure):
     _fields_ = [("num_blocks", ctypes.c_uint64), ("resident_blocks", ctypes.c_uint64),
                 ("resident_edge_bytes", ctypes.c_uint64), ("host_edge_bytes", ctypes.c_uint64),
-                ("device_bytes", ctypes.c_uint64)]
+                ("device_bytes", ctypes.c_uint64), ("small_list_degree", ctypes.c_uint64),
+                ("small_list_bytes", ctypes.c_uint64), ("small_list_vertices", ctypes.c_uint64)]
 
 
 class _GraphInfo(ctypes.Structure):
     _fields_ = [("nv", ctypes.c_uint64), ("ne", ctypes.c_uint64), ("fmt", ctypes.c_uint32),
                 ("esz", ctypes.c_uint32), ("device", ctypes.c_uint32),
-                ("weighted", ctypes.c_uint32)]
+                ("weighted", ctypes.c_uint32), ("mem_esz", ctypes.c_uint32),
+                ("weight_bits", ctypes.c_uint32)]
 
 
 class _RmatOpts(ctypes.Structure):
@@ -113,7 +115,7 @@ class _QueryStats(ctypes.Structure):
 # Every function include/thv.h declares (tests check the library exports them).
 ABI_FUNCTIONS = [
     "thv_open", "thv_from_arrays", "thv_generate_rmat", "thv_save", "thv_close",
-    "thv_info", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_run",
+    "thv_info", "thv_set_edge_packing", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_run",
     "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
     "thv_pick_sources", "thv_bfs_noalloc", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
@@ -141,6 +143,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_save": ([P, ctypes.c_char_p], I32),
         "thv_close": ([P], I32),
         "thv_info": ([P, ctypes.POINTER(_GraphInfo)], I32),
+        "thv_set_edge_packing": ([P, I32], I32),
         "thv_host_arrays": ([P, pp, pp, pp], I32),
         "thv_plan": ([P, ctypes.POINTER(_PlanOpts)], I32),
         "thv_get_plan": ([P, ctypes.POINTER(_PlanInfo)], I32),
@@ -190,11 +193,24 @@ class Graph:
 
     def __init__(self, handle: ctypes.c_void_p):
         self._h = handle
+        self._refresh()
+
+    def _refresh(self) -> None:
         info = _GraphInfo()
         _check(load_library().thv_info(self._h, ctypes.byref(info)), "thv_info")
         self.nv, self.ne = int(info.nv), int(info.ne)
         self.fmt = {v: k for k, v in FMT.items()}[info.fmt]
+        # esz: the format's bytes per edge; mem_esz: as stored (4 when packed)
         self.esz, self.weighted, self.device = int(info.esz), bool(info.weighted), int(info.device)
+        self.mem_esz, self.weight_bits = int(info.mem_esz), int(info.weight_bits)
+
+    def set_edge_packing(self, packed: bool) -> None:
+        """Store weighted edges packed in 4 bytes (default) or as {dst, w}
+        pairs; drops the plan.  Host views from host_arrays() are invalid
+        afterwards."""
+        _check(load_library().thv_set_edge_packing(self._h, 1 if packed else 0),
+               "thv_set_edge_packing")
+        self._refresh()
 
     # -- construction -------------------------------------------------------
     @classmethod
@@ -234,10 +250,13 @@ class Graph:
 
     # -- plan ---------------------------------------------------------------
     def plan(self, hbm_budget_bytes: Optional[int] = None, block_bytes: int = 0,
-             policy: str = "densest") -> dict:
+             policy: str = "densest", small_list_degree: int = 0) -> dict:
+        """Choose the HBM-resident edges.  small_list_degree: lists shorter
+        than this in host blocks are cached in HBM first (0 = default: 64
+        for CSR/WCSR, off for CSC; 1 = off; PageRank ignores the cache)."""
         lib = load_library()
         o = _PlanOpts(2**64 - 1 if hbm_budget_bytes is None else int(hbm_budget_bytes),
-                      int(block_bytes), PLACE[policy], 0)
+                      int(block_bytes), PLACE[policy], int(small_list_degree))
         _check(lib.thv_plan(self._h, ctypes.byref(o)), "thv_plan")
         return self.plan_info()
 

@@ -50,6 +50,7 @@ struct MsArgs {
   const uint32_t *blk_vb;
   const uint64_t *blk_base;
   uint64_t host_base;
+  ListCache lc;
   unsigned long long *visit;  // BFS
   unsigned long long *front;  // pending (vertex, source) pairs
   uint8_t *lvl;               // BFS [nv][64]: level + 1, 0 = unreached
@@ -63,7 +64,9 @@ struct MsArgs {
   const uint32_t *sources;  // [k, source 0, ..., source k-1]
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, max_iters;
-  uint32_t small_deg, chunk, delta, pad;
+  uint32_t small_deg, chunk, delta;
+  uint32_t wshift, wbase;  // packed weighted edges (see edge_dst / edge_wt)
+  uint32_t pad;
 };
 
 struct BatchState {
@@ -138,9 +141,10 @@ __device__ __forceinline__ void ms_sssp_edge(const MsArgs &a, uint32_t u, uint32
 }
 
 // Lane-per-source SSSP relaxation of one work item: the warp loads the
-// item's {dst, w} edges 32 at a time (coalesced) and relaxes each edge for
-// every source of the mask at once, lanes = sources, so dist[w][.] is read
-// as coalesced 128-byte lines; four edges' rows are in flight per step.
+// item's edges 32 at a time (coalesced) and relaxes each edge for every
+// source of the mask at once, lanes = sources, so dist[w][.] is read as
+// coalesced 128-byte lines; four edges' rows are in flight per step.
+template <int ESZ>
 __device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t u, uintptr_t eaddr,
                                              uint32_t cnt, unsigned long long f) {
   const unsigned lane = lane_id();
@@ -149,7 +153,15 @@ __device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t u, uintpt
   const uint32_t d0 = lo ? ldcg(du + lane) : 0u, d1 = hi ? ldcg(du + 32 + lane) : 0u;
   for (uint32_t base = 0; base < cnt; base += 32) {
     const uint32_t k = base + lane;
-    const uint2 e = k < cnt ? ld_nc_u2(eaddr + (uintptr_t)k * 8u) : make_uint2(0, 0);
+    uint2 e = make_uint2(0, 0);
+    if (k < cnt) {
+      if (ESZ == 8) {
+        e = ld_nc_u2(eaddr + (uintptr_t)k * 8u);
+      } else {
+        const uint32_t r = ld_nc_u32(eaddr + (uintptr_t)k * 4u);
+        e = make_uint2(edge_dst(r, a.wshift), edge_wt(r, a.wshift, a.wbase));
+      }
+    }
     const uint32_t m = min(32u, cnt - base);
     for (uint32_t j = 0; j < m; j += 4) {
       uint32_t w[4], wt[4], c0[4], c1[4];
@@ -206,7 +218,7 @@ template <int OP, int ESZ>
 __device__ __forceinline__ void ms_chunk(const MsArgs &a, const WorkItem &it,
                                          unsigned long long f, uint32_t lvl1) {
   if (OP == MS_SSSP && __popcll(f) > kSparseMask) {
-    ms_sssp_item(a, it.v, it.eaddr, it.cnt, f);
+    ms_sssp_item<ESZ>(a, it.v, it.eaddr, it.cnt, f);
     return;
   }
   constexpr int PER = 16 / ESZ;
@@ -220,7 +232,8 @@ __device__ __forceinline__ void ms_chunk(const MsArgs &a, const WorkItem &it,
     for (int j = 0; j < PER; j++) {
       const uintptr_t ea = p + (uintptr_t)ESZ * j;
       if (ea >= start && ea < end)
-        ms_edge<OP, ESZ>(a, it.v, ESZ == 4 ? e[j] : e[2 * j], ESZ == 4 ? 1u : e[2 * j + 1], f, lvl1);
+        ms_edge<OP, ESZ>(a, it.v, ESZ == 4 ? edge_dst(e[j], a.wshift) : e[2 * j],
+                         ESZ == 4 ? edge_wt(e[j], a.wshift, a.wbase) : e[2 * j + 1], f, lvl1);
     }
   }
 }
@@ -242,7 +255,7 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long fir
     while (dense) {
       const int i = __ffs(dense) - 1;
       dense &= dense - 1;
-      ms_sssp_item(a, __shfl_sync(kFull, it.v, i), (uintptr_t)shfl64(it.eaddr, i),
+      ms_sssp_item<ESZ>(a, __shfl_sync(kFull, it.v, i), (uintptr_t)shfl64(it.eaddr, i),
                    __shfl_sync(kFull, it.cnt, i), shfl64(f, i));
     }
     if (__popcll(f) > kSparseMask) {
@@ -263,7 +276,8 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long fir
     if (t < total) {
       const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
       if (ESZ == 4) {
-        ms_edge<OP, ESZ>(a, ou, ld_nc_u32(addr), 1u, of, lvl1);
+        const uint32_t r = ld_nc_u32(addr);
+        ms_edge<OP, ESZ>(a, ou, edge_dst(r, a.wshift), edge_wt(r, a.wshift, a.wbase), of, lvl1);
       } else {
         const uint2 e = ld_nc_u2(addr);
         ms_edge<OP, ESZ>(a, ou, e.x, e.y, of, lvl1);
@@ -356,12 +370,12 @@ __global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
         if (take) {
           const uint64_t s0 = __ldg(a.off + v), e0 = __ldg(a.off + v + 1);
           deg = (uint32_t)(e0 - s0);
-          const uint32_t b = find_block(vb, a.nblk, v);
-          const unsigned long long base = __ldg(a.blk_base + b);
-          eaddr = base + s0 * ESZ;
+          bool host;
+          eaddr = list_addr(a.lc, __ldg(a.blk_base + find_block(vb, a.nblk, v)), a.host_base, v,
+                            s0, deg, ESZ, &host);
           my_edges += deg;
           my_pairs += __popcll(take);
-          if (base == a.host_base) my_link += (unsigned long long)deg * ESZ;
+          if (host) my_link += (unsigned long long)deg * ESZ;
           else my_hbm += (unsigned long long)deg * ESZ;
         }
         const bool small = take && deg > 0 && deg < a.small_deg;
@@ -690,8 +704,9 @@ static thv_status enqueue_any(thv_graph *g, MsArgs &a, cudaStream_t st, bool wan
 static thv_status enqueue(thv_graph *g, bool sssp, MsArgs &a, cudaStream_t st, bool want_out,
                           uint32_t threads) {
   if (sssp) {
-    if (g->esz != 8) return fail(THV_EINVAL, "SSSP needs 8-byte weighted edges");
-    return enqueue_any<MS_SSSP, 8>(g, a, st, want_out, threads);
+    if (!g->weighted) return fail(THV_EINVAL, "SSSP needs edge weights");
+    return g->esz == 8 ? enqueue_any<MS_SSSP, 8>(g, a, st, want_out, threads)
+                       : enqueue_any<MS_SSSP, 4>(g, a, st, want_out, threads);  // packed
   }
   return g->esz == 8 ? enqueue_any<MS_BFS, 8>(g, a, st, want_out, threads)
                      : enqueue_any<MS_BFS, 4>(g, a, st, want_out, threads);
@@ -840,6 +855,9 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
   a.blk_vb = g->plan.d_vbegin;
   a.blk_base = g->plan.d_base;
   a.host_base = g->h_edges_dev;
+  a.lc = list_cache_of(g->plan);
+  a.wshift = g->wshift;
+  a.wbase = g->wbase;
   a.visit = b->d_visit;
   a.front = b->d_front;
   a.lvl = b->d_lvl;

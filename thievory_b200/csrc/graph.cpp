@@ -147,6 +147,84 @@ static thv_status validate(thv_graph *g) {
   return THV_OK;
 }
 
+static uint32_t bit_width(uint32_t x) { return x ? 32u - (uint32_t)__builtin_clz(x) : 0u; }
+
+// Weighted edges are stored in 4 bytes, dst << wshift | (w - wbase), when
+// the id bits and the bits of the weight range fit 32 (lossless); the
+// {dst, w} pairs are restored for save and the host view.
+thv_status set_packing(thv_graph *g, bool on) {
+  if (!g->weighted || on == g->packed) return THV_OK;
+  THV_CUDA(cudaSetDevice(g->device));
+  if (g->stream) THV_CUDA(cudaStreamSynchronize(g->stream));
+  batch_free(g);
+  minprop_free(g);
+  pagerank_free(g);
+  plan_free(g);
+  const uint64_t ne = g->ne;
+  const uint32_t *e = (const uint32_t *)g->h_edges;
+  void *nb = nullptr;
+  if (on) {
+    uint32_t wmin = 0xFFFFFFFFu, wmax = 0;
+#pragma omp parallel for schedule(static) reduction(min : wmin) reduction(max : wmax)
+    for (int64_t i = 0; i < (int64_t)ne; i++) {
+      wmin = std::min(wmin, e[2 * i + 1]);
+      wmax = std::max(wmax, e[2 * i + 1]);
+    }
+    if (!ne) wmin = wmax = 0;
+    const uint32_t ib = bit_width(g->nv ? (uint32_t)(g->nv - 1) : 0u);
+    const uint32_t wb = bit_width(wmax - wmin);
+    if (wb >= 32 || ib + wb > 32) return THV_OK;  // does not fit: keep pairs
+    const size_t bytes = ne * 4 + kEdgePad;
+    THV_TRY(pinned_alloc(&nb, bytes, "pinned packed edges"));
+    uint32_t *p = (uint32_t *)nb;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)ne; i++) p[i] = (e[2 * i] << wb) | (e[2 * i + 1] - wmin);
+    memset(p + ne, 0, kEdgePad);
+    g->esz = 4;
+    g->wshift = wb;
+    g->wbase = wmin;
+    g->h_edges_bytes = bytes;
+  } else {
+    const size_t bytes = ne * 8 + kEdgePad;
+    THV_TRY(pinned_alloc(&nb, bytes, "pinned edges"));
+    uint32_t *p = (uint32_t *)nb;
+    const uint32_t wb = g->wshift, base = g->wbase, mask = (1u << wb) - 1u;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)ne; i++) {
+      p[2 * i] = e[i] >> wb;
+      p[2 * i + 1] = (e[i] & mask) + base;
+    }
+    memset(p + 2 * ne, 0, kEdgePad);
+    g->esz = 8;
+    g->wshift = g->wbase = 0;
+    g->h_edges_bytes = bytes;
+  }
+  pinned_free(g->h_edges);
+  g->h_edges = nb;
+  g->packed = on;
+  g->h_unpacked.clear();
+  g->h_unpacked.shrink_to_fit();
+  void *dp = nullptr;
+  THV_CUDA(cudaHostGetDevicePointer(&dp, g->h_edges, 0));
+  g->h_edges_dev = (uint64_t)dp;
+  return THV_OK;
+}
+
+// {dst, w} of edge i whatever the in-memory layout.
+static inline void edge_at(const thv_graph *g, uint64_t i, uint32_t *dst, uint32_t *w) {
+  const uint32_t *e = (const uint32_t *)g->h_edges;
+  if (g->packed) {
+    *dst = e[i] >> g->wshift;
+    *w = (e[i] & ((1u << g->wshift) - 1u)) + g->wbase;
+  } else if (g->esz == 8) {
+    *dst = e[2 * i];
+    *w = e[2 * i + 1];
+  } else {
+    *dst = e[i];
+    *w = 20u;  // converter.cpp writes weight 20 for unweighted inputs
+  }
+}
+
 static thv_status alloc_host_edges(thv_graph *g) {
   g->h_edges_bytes = g->ne * g->esz + kEdgePad;
   THV_TRY(pinned_alloc(&g->h_edges, g->h_edges_bytes, "pinned edges"));
@@ -227,6 +305,7 @@ static thv_status open_file(const char *path, thv_format fmt, uint32_t flags,
   }
   THV_TRY(validate(g.get()));
   THV_TRY(graph_init_device(g.get()));
+  THV_TRY(set_packing(g.get(), true));
   *out = g.release();
   return THV_OK;
 }
@@ -236,6 +315,8 @@ static thv_status open_file(const char *path, thv_format fmt, uint32_t flags,
 void plan_free(thv_graph *g) {
   Plan &p = g->plan;
   dev_free(p.d_resident);
+  dev_free(p.d_lists);
+  dev_free(p.d_list_idx);
   dev_free(p.d_vbegin);
   dev_free(p.d_base);
   dev_free(p.d_tiles);
@@ -243,9 +324,78 @@ void plan_free(thv_graph *g) {
   p = Plan();
 }
 
+// Packs the lists with 0 < deg < ldeg of every host block into d_lists, in
+// vertex order, through a pinned staging buffer.
+static thv_status build_list_cache(thv_graph *g, uint32_t ldeg) {
+  Plan &p = g->plan;
+  p.list_deg = ldeg;
+  if (!ldeg) return THV_OK;
+  const uint64_t esz = g->esz;
+  std::vector<uint32_t> idx(g->nv, 0);
+  uint64_t cursor = 0, verts = 0;
+  for (const Block &b : p.blocks) {
+    if (b.resident) continue;
+    for (uint64_t v = b.vbegin; v < b.vend; v++) {
+      const uint64_t d = g->off[v + 1] - g->off[v];
+      if (d > 0 && d < ldeg) {
+        idx[v] = (uint32_t)cursor;
+        cursor += d;
+        verts++;
+      }
+    }
+  }
+  p.list_bytes = cursor * esz;
+  p.list_vertices = verts;
+  if (!cursor) {
+    p.list_deg = 0;
+    return THV_OK;
+  }
+  p.d_lists_bytes = kListLead + cursor * esz + kEdgePad;
+  THV_TRY(dev_alloc((void **)&p.d_lists, p.d_lists_bytes, "small-list cache"));
+  THV_TRY(dev_alloc((void **)&p.d_list_idx, g->nv * 4, "small-list index"));
+  THV_CUDA(cudaMemset(p.d_lists, 0, p.d_lists_bytes));
+  THV_CUDA(cudaMemcpy(p.d_list_idx, idx.data(), g->nv * 4, cudaMemcpyHostToDevice));
+  // stage vertex ranges of at most kStage bytes; lists are copied in parallel
+  constexpr uint64_t kStage = 64ull << 20;
+  char *stage = nullptr;
+  THV_TRY(pinned_alloc((void **)&stage, kStage, "list staging"));
+  std::vector<uint32_t> vs;  // cached vertices in cache order
+  vs.reserve(verts);
+  for (const Block &b : p.blocks) {
+    if (b.resident) continue;
+    for (uint64_t v = b.vbegin; v < b.vend; v++) {
+      const uint64_t d = g->off[v + 1] - g->off[v];
+      if (d > 0 && d < ldeg) vs.push_back((uint32_t)v);
+    }
+  }
+  thv_status st = THV_OK;
+  const char *src = (const char *)g->h_edges;
+  for (size_t i = 0; i < vs.size() && st == THV_OK;) {
+    const uint64_t e0 = idx[vs[i]];
+    size_t j = i;
+    while (j < vs.size() && (idx[vs[j]] - e0 + (g->off[vs[j] + 1] - g->off[vs[j]])) * esz <= kStage)
+      j++;
+#pragma omp parallel for schedule(static, 4096)
+    for (size_t k = i; k < j; k++) {
+      const uint32_t v = vs[k];
+      memcpy(stage + (idx[v] - e0) * esz, src + g->off[v] * esz,
+             (g->off[v + 1] - g->off[v]) * esz);
+    }
+    const uint64_t last = vs[j - 1];
+    const uint64_t bytes = (idx[last] - e0 + (g->off[last + 1] - g->off[last])) * esz;
+    if (cudaMemcpy(p.d_lists + kListLead + e0 * esz, stage, bytes, cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      st = fail(THV_ECUDA, "small-list cache copy failed");
+    i = j;
+  }
+  pinned_free(stage);
+  return st;
+}
+
 static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
   THV_CUDA(cudaSetDevice(g->device));
   if (g->stream) THV_CUDA(cudaStreamSynchronize(g->stream));
+  batch_free(g);  // its captured launch graphs hold the old plan's tables
   plan_free(g);
   Plan &p = g->plan;
   const uint64_t esz = g->esz;
@@ -275,6 +425,40 @@ static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
     budget = fr > reserve ? std::min<uint64_t>(total, fr - reserve) : 0;
   }
   p.budget_bytes = budget;
+  // Small-list cache threshold: the largest t <= the requested one whose
+  // lists (0 < deg < t) fit the budget and 2^32 cached elements.
+  uint32_t ldeg = o && o->small_list_degree ? o->small_list_degree
+                                            : (g->fmt == THV_FMT_CSC ? 1u : kDefaultListDeg);
+  ldeg = (uint32_t)std::min<uint64_t>(ldeg, g->nv + 1);
+  if (ldeg > 1) {
+    std::vector<uint64_t> by_deg(ldeg, 0);  // edges in lists of each degree
+    for (uint64_t v = 0; v < g->nv; v++) {
+      const uint64_t d = g->off[v + 1] - g->off[v];
+      if (d > 0 && d < ldeg) by_deg[d] += d;
+    }
+    uint64_t acc = 0;
+    uint32_t t = 1;
+    while (t < ldeg && (acc + by_deg[t]) * esz <= budget && acc + by_deg[t] < (1ull << 32)) {
+      acc += by_deg[t];
+      t++;
+    }
+    ldeg = t;
+  }
+  if (ldeg <= 1) ldeg = 0;
+  // per-block bytes of small lists; a resident block needs none of them cached
+  std::vector<uint64_t> small_b(p.blocks.size(), 0);
+  uint64_t small_total = 0;
+  if (ldeg) {
+    for (size_t b = 0; b < p.blocks.size(); b++) {
+      uint64_t s = 0;
+      for (uint64_t v = p.blocks[b].vbegin; v < p.blocks[b].vend; v++) {
+        const uint64_t d = g->off[v + 1] - g->off[v];
+        if (d > 0 && d < ldeg) s += d;
+      }
+      small_b[b] = s * esz;
+      small_total += s * esz;
+    }
+  }
   std::vector<uint32_t> order(p.blocks.size());
   std::iota(order.begin(), order.end(), 0u);
   if (p.policy == THV_PLACE_DENSEST) {
@@ -286,13 +470,15 @@ static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
       return l > r;
     });
   }
-  uint64_t used = 0;
+  // the cache is paid first; a block then costs only its long lists
+  uint64_t used = small_total;
   for (uint32_t b : order) {
     const uint64_t bytes = (p.blocks[b].eend - p.blocks[b].ebegin) * esz;
     if (bytes == 0) continue;
-    if (used + bytes <= budget) {
+    const uint64_t cost = bytes - small_b[b];
+    if (used + cost <= budget) {
       p.blocks[b].resident = true;
-      used += bytes;
+      used += cost;
     } else if (p.policy == THV_PLACE_PREFIX) {
       break;
     }
@@ -317,6 +503,7 @@ static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
                           (b.eend - b.ebegin) * esz, cudaMemcpyHostToDevice));
     }
   }
+  THV_TRY(build_list_cache(g, ldeg));
   p.resident_edge_bytes = used;
   p.host_edge_bytes = total - used;
   const size_t nb = p.blocks.size();
@@ -427,6 +614,7 @@ static thv_status from_arrays(uint64_t nv, uint64_t ne, const uint64_t *off,
   if (fmt == THV_FMT_CSC) g->outdeg.assign(outdeg, outdeg + nv);
   THV_TRY(validate(g.get()));
   THV_TRY(graph_init_device(g.get()));
+  THV_TRY(set_packing(g.get(), true));
   *out = g.release();
   return THV_OK;
 }
@@ -447,6 +635,7 @@ thv_status graph_adopt(uint64_t nv, uint64_t ne, thv_format fmt, uint32_t esz,
   THV_TRY(alloc_host_edges(g.get()));
   if (ne) THV_CUDA(cudaMemcpy(g->h_edges, d_edges, ne * esz, cudaMemcpyDeviceToHost));
   THV_TRY(graph_init_device(g.get()));
+  THV_TRY(set_packing(g.get(), true));
   *out = g.release();
   return THV_OK;
 }
@@ -456,33 +645,33 @@ static thv_status save(const thv_graph *g, const char *path) {
   if (!f) return fail(THV_EIO, "cannot create %s: %s", path, strerror(errno));
   bool ok = fwrite(&g->nv, 8, 1, f.get()) == 1 && fwrite(&g->ne, 8, 1, f.get()) == 1;
   ok = ok && (g->nv == 0 || fwrite(g->off.data(), 8, g->nv, f.get()) == g->nv);
-  const uint32_t *e = (const uint32_t *)g->h_edges;
   const uint64_t ne = g->ne;
+  std::vector<uint32_t> buf;
+  buf.reserve(1 << 20);
+  auto flush = [&]() {
+    ok = ok && (buf.empty() || fwrite(buf.data(), 4, buf.size(), f.get()) == buf.size());
+    buf.clear();
+  };
+  uint32_t d, w;
   if (g->fmt == THV_FMT_WCSR) {
-    if (g->esz == 8) {
-      ok = ok && (ne == 0 || fwrite(e, 8, ne, f.get()) == ne);
-    } else {
-      for (uint64_t i = 0; ok && i < ne; i++) {
-        const uint32_t pr[2] = {e[i], 20u};
-        ok = fwrite(pr, 4, 2, f.get()) == 2;
-      }
-    }
-  } else {
-    const uint32_t stride = g->esz / 4;
-    std::vector<uint32_t> buf;
-    buf.reserve(1 << 20);
-    auto flush = [&]() {
-      ok = ok && (buf.empty() || fwrite(buf.data(), 4, buf.size(), f.get()) == buf.size());
-      buf.clear();
-    };
     for (uint64_t i = 0; ok && i < ne; i++) {
-      buf.push_back(e[i * stride]);
+      edge_at(g, i, &d, &w);
+      buf.push_back(d);
+      buf.push_back(w);
+      if (buf.size() >= (1u << 20)) flush();
+    }
+    flush();
+  } else {
+    for (uint64_t i = 0; ok && i < ne; i++) {
+      edge_at(g, i, &d, &w);
+      buf.push_back(d);
       if (buf.size() == (1u << 20)) flush();
     }
     flush();
     if (g->fmt == THV_FMT_CSR) {  // trailing weight section
       for (uint64_t i = 0; ok && i < ne; i++) {
-        buf.push_back(g->esz == 8 ? e[2 * i + 1] : 20u);
+        edge_at(g, i, &d, &w);
+        buf.push_back(w);
         if (buf.size() == (1u << 20)) flush();
       }
       flush();
@@ -560,17 +749,32 @@ thv_status thv_info(const thv_graph *g, thv_graph_info *o) {
   o->nv = g->nv;
   o->ne = g->ne;
   o->fmt = g->fmt;
-  o->esz = g->esz;
+  o->esz = g->packed ? 8 : g->esz;
   o->device = (uint32_t)g->device;
   o->weighted = g->weighted;
+  o->mem_esz = g->esz;
+  o->weight_bits = g->packed ? g->wshift : 0;
   return THV_OK;
+}
+
+thv_status thv_set_edge_packing(thv_graph *g, int packed) {
+  THV_GUARD_BEGIN
+  if (!g) return fail(THV_EINVAL, "null graph");
+  return set_packing(g, packed != 0);
+  THV_GUARD_END
 }
 
 thv_status thv_host_arrays(const thv_graph *g, const uint64_t **off,
                            const void **edges, const uint32_t **outdeg) {
   if (!g) return fail(THV_EINVAL, "null argument");
   if (off) *off = g->off.data();
-  if (edges) *edges = g->h_edges;
+  if (edges && g->packed && g->h_unpacked.size() != 2 * g->ne) {
+    g->h_unpacked.resize(2 * g->ne);
+    uint32_t *u = g->h_unpacked.data();
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)g->ne; i++) edge_at(g, i, &u[2 * i], &u[2 * i + 1]);
+  }
+  if (edges) *edges = g->packed ? (const void *)g->h_unpacked.data() : g->h_edges;
   if (outdeg) *outdeg = g->fmt == THV_FMT_CSC ? g->outdeg.data() : nullptr;
   return THV_OK;
 }
@@ -591,7 +795,11 @@ thv_status thv_get_plan(const thv_graph *g, thv_plan_info *o) {
   for (const Block &b : p.blocks) o->resident_blocks += b.resident;
   o->resident_edge_bytes = p.resident_edge_bytes;
   o->host_edge_bytes = p.host_edge_bytes;
-  o->device_bytes = g->device_bytes + p.d_resident_bytes;
+  o->device_bytes = g->device_bytes + p.d_resident_bytes +
+                    (p.d_lists ? p.d_lists_bytes + g->nv * 4 : 0);
+  o->small_list_degree = p.list_deg;
+  o->small_list_bytes = p.list_bytes;
+  o->small_list_vertices = p.list_vertices;
   return THV_OK;
 }
 

@@ -127,6 +127,8 @@ int main(int argc, char **argv) {
   po.hbm_budget_bytes = UINT64_MAX;
   po.block_bytes = 0;
   po.policy = placement == "prefix" ? THV_PLACE_PREFIX : THV_PLACE_DENSEST;
+  // PageRank reads whole blocks: give the whole budget to blocks
+  if (a == THV_ALGO_PR_PULL || a == THV_ALGO_PR_PUSH) po.small_list_degree = 1;
   const uint64_t edge_bytes = info.ne * info.esz;
   if (!budget.empty() && !parse_size(budget.c_str(), edge_bytes, &po.hbm_budget_bytes)) {
     fprintf(stderr, "Error: bad --hbm-budget %s\n", budget.c_str());
@@ -146,6 +148,10 @@ int main(int argc, char **argv) {
          (unsigned long long)pi.num_blocks, (unsigned long long)pi.resident_blocks);
   printf("Resident edge bytes: %llu, host (zero-copy) edge bytes: %llu\n",
          (unsigned long long)pi.resident_edge_bytes, (unsigned long long)pi.host_edge_bytes);
+  if (pi.small_list_degree)
+    printf("Small lists (degree < %llu) cached in HBM: %llu vertices, %llu bytes\n",
+           (unsigned long long)pi.small_list_degree, (unsigned long long)pi.small_list_vertices,
+           (unsigned long long)pi.small_list_bytes);
 
   thv_run_opts ro{};
   ro.source = source;

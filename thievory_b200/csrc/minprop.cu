@@ -52,6 +52,7 @@ constexpr uint32_t kDefaultChunk = 256; // edges per high-degree work item
 // width 8 re-reads 5% more adjacency in ~80 iterations and is fastest.
 constexpr uint32_t kDefaultDelta = 8;
 constexpr uint32_t kCcGrowth = 8;       // CC label window growth per advance
+constexpr uint32_t kSsspGrowth = 1;     // SSSP window growth per advance
 
 
 // Frontier work item of the single-source engine: the adjacency of vertex v
@@ -85,17 +86,20 @@ struct MinArgs {
   const uint64_t *off;
   const uint32_t *blk_vb;
   const uint64_t *blk_base;
-  uint64_t host_base;
+  uint64_t host_base, host_end;  // zero-copy edge range [host_base, host_end)
+  ListCache lc;
   MinItem *qs, *qb;
   unsigned long long cap_s, cap_b;
   MinCtrl *ctrl;
-  // queue mode: second queue buffers and the "queued" bitmap
+  // queue mode: second queue buffers and the per-vertex queue tags
   MinItem *qs2, *qb2;
-  uint32_t *qd;
+  uint32_t *qtag;
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, max_iters;
   uint32_t delta, small_deg, chunk, src;
-  uint32_t growth, pad;
+  uint32_t growth;
+  uint32_t wshift, wbase;  // packed weighted edges (see edge_dst / edge_wt)
+  uint32_t pad;
 };
 
 struct MinState {
@@ -105,7 +109,7 @@ struct MinState {
   uint32_t *d_wmin = nullptr;
   MinItem *d_qs = nullptr, *d_qb = nullptr;
   MinItem *d_qs2 = nullptr, *d_qb2 = nullptr;
-  uint32_t *d_qd = nullptr;
+  uint32_t *d_qtag = nullptr;
   uint64_t cap_s = 0, cap_b = 0;
   uint32_t chunk = 0, small = 0;
   MinCtrl *d_ctrl = nullptr;
@@ -175,8 +179,8 @@ __device__ __forceinline__ void process_chunk(const MinArgs &a, const MinItem &i
         const uintptr_t ea = ph + (uintptr_t)ESZ * j;
         const int k = h * PER + j;
         ok[k] = (h == 0 || second) && ea >= start && ea < end;
-        w[k] = ESZ == 4 ? f[j] : f[2 * j];
-        cand[k] = candidate<OP>(vval, ESZ == 4 ? 0u : f[2 * j + 1]);
+        w[k] = ESZ == 4 ? edge_dst(f[j], a.wshift) : f[2 * j];
+        cand[k] = candidate<OP>(vval, ESZ == 4 ? edge_wt(f[j], a.wshift, a.wbase) : f[2 * j + 1]);
       }
     }
     relax_n<OP, 2 * PER>(a, w, cand, ok);
@@ -218,7 +222,9 @@ __device__ __forceinline__ void process_group(const MinArgs &a, unsigned long lo
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       if (ESZ == 4) {
-        w[h] = ok[h] ? ld_nc_u32(addr[h]) : 0u;
+        const uint32_t e = ok[h] ? ld_nc_u32(addr[h]) : 0u;
+        w[h] = edge_dst(e, a.wshift);
+        wt[h] = edge_wt(e, a.wshift, a.wbase);
       } else {
         const uint2 e = ok[h] ? ld_nc_u2(addr[h]) : make_uint2(0, 0);
         w[h] = e.x;
@@ -322,11 +328,12 @@ __global__ void __launch_bounds__(kMinThreads)
           if (OP == OP_BFS) vval = ldcg(a.val + v);
           const uint64_t s = __ldg(a.off + v), e = __ldg(a.off + v + 1);
           deg = (uint32_t)(e - s);
-          const unsigned long long base = bbase[find_block(vb, a.nblk, v)];
-          eaddr = base + s * ESZ;
+          bool host;
+          eaddr = list_addr(a.lc, bbase[find_block(vb, a.nblk, v)], a.host_base, v, s, deg, ESZ,
+                            &host);
           my_edges += deg;
           my_verts += 1;
-          if (base == a.host_base) my_link += (unsigned long long)deg * ESZ;
+          if (host) my_link += (unsigned long long)deg * ESZ;
           else my_hbm += (unsigned long long)deg * ESZ;
         }
         const bool small = take && deg > 0 && deg < a.small_deg;
@@ -391,7 +398,7 @@ __global__ void __launch_bounds__(kMinThreads)
       if (OP == OP_BFS) break;
       if (ldcg(&c->remaining[slot]) == 0) break;
       const uint32_t mk = ldcg(&c->minkept[slot]);
-      if (OP == OP_CC) width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
+      width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
       thr = (uint32_t)min((unsigned long long)mk + width, 0xFFFFFFFFull);
       continue;
     }
@@ -458,19 +465,30 @@ __global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
 // The bitmap scan runs only when the near queue is empty: at the start, and
 // when an SSSP/CC window advances over vertices parked in the far bitmap.
 //
-// SSSP/CC push once per queue through a "queued" bit.  Ordering: the pusher
-// does atomicMin(val); fence.sc; atomicOr(queued) and pushes only if the bit
-// was clear; the expander does atomicAnd(queued, ~bit); fence.sc; load val.
-// With sequentially consistent fences on both sides at least one of them
-// sees the other: either the expansion reads the lowered value, or the
-// pusher sees the bit cleared and queues the vertex again -- no decrease is
-// lost.  BFS needs neither: a vertex changes once, its pusher is unique.
-
-__device__ __forceinline__ void fence_sc() { asm volatile("fence.sc.gpu;" ::: "memory"); }
+// SSSP/CC push a vertex at most once per queue through a per-vertex tag:
+// phase ph appends to its output queue with tag ph + 1, and a relaxation that
+// lowers w below the window pushes it only if atomicMax(tag[w], ph + 1) saw a
+// smaller tag.  Invariant: tag[w] == ph + 1 implies w has an entry in phase
+// ph's output queue, which the next phase expands after a grid barrier and
+// so with the final value of this phase.  The expander of phase ph therefore
+// skips an entry whose tag already reads ph + 1 (it is queued again, with a
+// lower value); otherwise it expands with the value it reads.  No decrease is
+// lost under any ordering of the two sides, so no fence is needed; a late
+// tag read only costs a redundant expansion.  BFS needs no tags: a vertex
+// changes once and its pusher is unique.
 
 struct QStats {
-  unsigned long long edges = 0, hbm = 0, link = 0, verts = 0;
+  unsigned long long edges = 0, hbm = 0, link = 0;
 };
+
+// Expansion accounting: edge count and bytes by where the edges live.
+__device__ __forceinline__ void q_count(const MinArgs &a, QStats &qst, unsigned long long eaddr,
+                                        unsigned cnt, unsigned esz) {
+  qst.edges += cnt;
+  const unsigned long long b = (unsigned long long)cnt * esz;
+  if (eaddr >= a.host_base && eaddr < a.host_end) qst.link += b;  // cache lies outside
+  else qst.hbm += b;
+}
 
 // Warp-uniform: lanes with `flag` append vertex w (value wval) to the queue
 // pair (qs, qb) whose counters live in slot cs.
@@ -487,12 +505,9 @@ __device__ __forceinline__ void q_append(const MinArgs &a, const uint32_t *vb,
   if (flag) {
     const uint64_t s0 = __ldg(a.off + w), e0 = __ldg(a.off + w + 1);
     deg = (uint32_t)(e0 - s0);
-    const unsigned long long base = bbase[find_block(vb, a.nblk, w)];
-    eaddr = base + s0 * ESZ;
-    qst.edges += deg;
-    qst.verts += 1;
-    if (base == a.host_base) qst.link += (unsigned long long)deg * ESZ;
-    else qst.hbm += (unsigned long long)deg * ESZ;
+    bool host;
+    eaddr = list_addr(a.lc, bbase[find_block(vb, a.nblk, w)], a.host_base, w, s0, deg, ESZ,
+                      &host);
   }
   const bool small = flag && deg > 0 && deg < a.small_deg;
   const bool big = flag && deg >= a.small_deg;
@@ -534,6 +549,7 @@ struct QEnv {
   MinItem *qs_next, *qb_next;
   unsigned cs_next;
   uint32_t thr;
+  uint32_t tag;  // tag of the output queue: phase + 1
 };
 
 // Relax N edges per lane; near improvements are queued, far ones parked.
@@ -554,9 +570,7 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
         if (OP == OP_BFS) {
           push[j] = true;
         } else if (cand[j] < e.thr) {
-          fence_sc();
-          const uint32_t m = 1u << (w[j] & 31u);
-          push[j] = !(atomicOr(a.qd + (w[j] >> 5), m) & m);
+          push[j] = ldcg(a.qtag + w[j]) != e.tag && atomicMax(a.qtag + w[j], e.tag) < e.tag;
         } else {
           atomicMin(a.wmin + (w[j] >> 5), (uint32_t)cand[j]);
           const uint32_t m = 1u << (w[j] & 31u);
@@ -572,19 +586,19 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
                   (uint32_t)cand[j], qst);
 }
 
-// Value of a dequeued vertex: BFS values are final when queued; SSSP/CC
-// clear the vertex's queued and parked bits, fence, then read the latest.
+// Dequeue: BFS values are final when queued.  SSSP/CC clear the vertex's
+// parked bit (its pending value is handled here), read the latest value and
+// report a skip when the vertex is already queued again for the next phase.
 template <int OP>
-__device__ __forceinline__ uint32_t q_dequeue(const MinArgs &a, bool valid, uint32_t v,
-                                              uint32_t item_val) {
+__device__ __forceinline__ uint32_t q_dequeue(const MinArgs &a, const QEnv &e, uint32_t v,
+                                              uint32_t item_val, bool &skip) {
+  skip = false;
   if (OP == OP_BFS) return item_val;
   const uint32_t m = 1u << (v & 31u);
-  if (valid) {
-    atomicAnd(a.qd + (v >> 5), ~m);
-    if (ldcg(a.bm + (v >> 5)) & m) atomicAnd(a.bm + (v >> 5), ~m);
-  }
-  fence_sc();
-  return valid ? ldcg(a.val + v) : 0u;
+  if (ldcg(a.bm + (v >> 5)) & m) atomicAnd(a.bm + (v >> 5), ~m);
+  const uint32_t cur = ldcg(a.val + v);
+  skip = ldcg(a.qtag + v) == e.tag;
+  return cur;
 }
 
 template <int OP, int ESZ>
@@ -592,11 +606,16 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
                                         QStats &qst) {
   constexpr int PER = 16 / ESZ;
   const unsigned lane = lane_id();
-  uint32_t vval = 0;
-  if (OP == OP_BFS) vval = it.val;
-  else vval = __shfl_sync(kFull, q_dequeue<OP>(a, lane == 0, it.v, it.val), 0);
+  uint32_t vval = it.val;
+  if (OP != OP_BFS) {
+    bool skip = false;
+    if (lane == 0) vval = q_dequeue<OP>(a, e, it.v, it.val, skip);
+    vval = __shfl_sync(kFull, vval, 0);
+    if (__shfl_sync(kFull, skip, 0)) return;
+  }
   const uintptr_t start = it.ea_cnt & kAddrMask;
   const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
+  if (lane == 0) q_count(a, qst, start, (unsigned)(it.ea_cnt >> 48), ESZ);
   for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; __any_sync(kFull, p < end); p += 512u) {
     const bool in = p < end;
     const uint4 q = in ? ld_nc_v4(p) : make_uint4(0, 0, 0, 0);
@@ -608,8 +627,8 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
     for (int j = 0; j < PER; j++) {
       const uintptr_t ea = p + (uintptr_t)ESZ * j;
       ok[j] = in && ea >= start && ea < end;
-      w[j] = ESZ == 4 ? f[j] : f[2 * j];
-      cand[j] = candidate<OP>(vval, ESZ == 4 ? 0u : f[2 * j + 1]);
+      w[j] = ESZ == 4 ? edge_dst(f[j], a.wshift) : f[2 * j];
+      cand[j] = candidate<OP>(vval, ESZ == 4 ? edge_wt(f[j], a.wshift, a.wbase) : f[2 * j + 1]);
     }
     q_relax_n<OP, ESZ, PER>(a, e, w, cand, ok, qst);
   }
@@ -624,9 +643,12 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
   MinItem it{0, 0, 0};
   const bool valid = idx < n_small;
   if (valid) it = qs[idx];
-  const uint32_t vval = q_dequeue<OP>(a, valid, it.v, it.val);
-  const unsigned cnt = (unsigned)(it.ea_cnt >> 48);
+  bool skip = !valid;
+  uint32_t vval = 0;
+  if (valid) vval = q_dequeue<OP>(a, e, it.v, it.val, skip);
+  const unsigned cnt = skip ? 0u : (unsigned)(it.ea_cnt >> 48);
   const unsigned long long eaddr = it.ea_cnt & kAddrMask;
+  if (cnt) q_count(a, qst, eaddr, cnt, ESZ);
   const unsigned incl = warp_incl_scan<unsigned>(cnt);
   const unsigned excl = incl - cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
@@ -643,7 +665,9 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
     if (ok[0]) {
       const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
       if (ESZ == 4) {
-        w[0] = ld_nc_u32(addr);
+        const uint32_t ed = ld_nc_u32(addr);
+        w[0] = edge_dst(ed, a.wshift);
+        wt = edge_wt(ed, a.wshift, a.wbase);
       } else {
         const uint2 ed = ld_nc_u2(addr);
         w[0] = ed.x;
@@ -656,7 +680,8 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
 }
 
 template <int OP, int ESZ>
-__global__ void __launch_bounds__(kMinThreads) minq_kernel(MinArgs a) {
+// Two blocks per SM: 64 registers, no spills (3 blocks spill and measured slower).
+__global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
   extern __shared__ unsigned long long s_tab[];
   const bool smem_tab = a.nblk <= kSmemBlocks;
   unsigned long long *s_base = s_tab;
@@ -706,6 +731,7 @@ __global__ void __launch_bounds__(kMinThreads) minq_kernel(MinArgs a) {
     env.qb_next = qb_out;
     env.cs_next = cur;
     env.thr = thr;
+    env.tag = ph + 1;
     if (scan) {
       // ------------------------------------------------------------- scan
       unsigned long long my_keep = 0;
@@ -737,7 +763,6 @@ __global__ void __launch_bounds__(kMinThreads) minq_kernel(MinArgs a) {
             if (lane == 0) {
               my_keep += __popc(wd & ~tm);
               a.wmin[wbase + j] = kmin;
-              if (tm) atomicOr(a.qd + wbase + j, tm);
             }
           }
           if (lane == 0 && tm) a.bm[wbase + j] = wd & ~tm;
@@ -778,27 +803,24 @@ __global__ void __launch_bounds__(kMinThreads) minq_kernel(MinArgs a) {
     } else {
       if (OP == OP_BFS || ldcg(&c->remaining[cur]) == 0) break;
       const uint32_t mk = ldcg(&c->minkept[cur]);
-      if (OP == OP_CC) width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
+      width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
       thr = (uint32_t)min((unsigned long long)mk + width, 0xFFFFFFFFull);
     }
   }
   qst.edges = warp_sum(qst.edges);
   qst.hbm = warp_sum(qst.hbm);
   qst.link = warp_sum(qst.link);
-  qst.verts = warp_sum(qst.verts);
-  if (lane == 0 && qst.verts) {
+  if (lane == 0 && qst.edges) {
     atomicAdd(&c->edges, qst.edges);
     atomicAdd(&c->hbm_bytes, qst.hbm);
     atomicAdd(&c->link_bytes, qst.link);
-    atomicAdd(&c->vertices, qst.verts);
   }
   if (leader) c->iters = iter;
 }
 
-template <int OP>
-__global__ void minq_clear(uint32_t *qd, uint32_t nw_alloc) {
-  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nw_alloc; w += gridDim.x * blockDim.x)
-    qd[w] = 0;
+__global__ void minq_clear(uint32_t *qtag, uint32_t nv) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
+    qtag[v] = 0;
 }
 
 __global__ void values_checksum_kernel(const uint32_t *val, uint64_t nv,
@@ -847,7 +869,7 @@ static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
   THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(MinItem), "chunk queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qs2, ms->cap_s * sizeof(MinItem), "queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qb2, ms->cap_b * sizeof(MinItem), "chunk queue"));
-  THV_TRY(dev_alloc((void **)&ms->d_qd, nw_alloc * 4, "queued bitmap"));
+  THV_TRY(dev_alloc((void **)&ms->d_qtag, g->nv * 4 + 64, "queue tags"));
   THV_TRY(dev_alloc((void **)&ms->d_ctrl, sizeof(MinCtrl), "control"));
   THV_TRY(pinned_alloc((void **)&ms->h_ctrl, sizeof(MinCtrl), "control"));
   THV_CUDA(cudaEventCreate(&ms->ev0));
@@ -866,7 +888,7 @@ void minprop_free(thv_graph *g) {
   dev_free(ms->d_qb);
   dev_free(ms->d_qs2);
   dev_free(ms->d_qb2);
-  dev_free(ms->d_qd);
+  dev_free(ms->d_qtag);
   dev_free(ms->d_ctrl);
   pinned_free(ms->h_ctrl);
   if (ms->ev0) cudaEventDestroy(ms->ev0);
@@ -890,8 +912,8 @@ static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
   const int init_grid = std::max(1, std::min<int>(g->num_sms * 8,
                                 (int)((g->nv + 255) / 256)));
   minprop_init<OP><<<init_grid, 256, 0, st>>>(a, nw_alloc);
-  if (!scan_mode) {
-    minq_clear<OP><<<init_grid, 256, 0, st>>>(a.qd, nw_alloc);
+  if (!scan_mode && OP != OP_BFS) {
+    minq_clear<<<init_grid, 256, 0, st>>>(a.qtag, a.nv);
     launches++;
   }
   THV_CUDA(cudaGetLastError());
@@ -937,11 +959,13 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.blk_vb = g->plan.d_vbegin;
   a.blk_base = g->plan.d_base;
   a.host_base = g->h_edges_dev;
+  a.host_end = g->h_edges_dev + g->h_edges_bytes;
+  a.lc = list_cache_of(g->plan);
   a.qs = ms->d_qs;
   a.qb = ms->d_qb;
   a.qs2 = ms->d_qs2;
   a.qb2 = ms->d_qb2;
-  a.qd = ms->d_qd;
+  a.qtag = ms->d_qtag;
   a.cap_s = ms->cap_s;
   a.cap_b = ms->cap_b;
   a.ctrl = ms->d_ctrl;
@@ -952,7 +976,9 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.ngroups = ms->ngroups;
   a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0xFFFFFFF0ull) * 2 + 8;
   a.delta = o && o->sssp_delta ? o->sssp_delta : (op == OP_CC ? 1u : kDefaultDelta);
-  a.growth = kCcGrowth;
+  a.growth = op == OP_CC ? kCcGrowth : kSsspGrowth;
+  a.wshift = g->wshift;
+  a.wbase = g->wbase;
   a.small_deg = small;
   a.chunk = chunk;
   a.src = src;
@@ -968,7 +994,7 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   if (g->esz == 4) {
     if (op == OP_BFS) s = launch_minprop<OP_BFS, 4>(g, a, st, launches, scan_mode);
     else if (op == OP_CC) s = launch_minprop<OP_CC, 4>(g, a, st, launches, scan_mode);
-    else s = fail(THV_EINVAL, "SSSP needs 8-byte weighted edges");
+    else s = launch_minprop<OP_SSSP, 4>(g, a, st, launches, scan_mode);  // packed weights
   } else {
     if (op == OP_BFS) s = launch_minprop<OP_BFS, 8>(g, a, st, launches, scan_mode);
     else if (op == OP_CC) s = launch_minprop<OP_CC, 8>(g, a, st, launches, scan_mode);
@@ -1128,6 +1154,7 @@ static thv_status bfs_noalloc(const uint64_t *d_off, const uint32_t *d_adj, uint
   a.blk_vb = (const uint32_t *)(base + l.table_vb);
   a.blk_base = (const uint64_t *)(base + l.table_base);
   a.host_base = 0;
+  a.host_end = 0;
   a.qs = (MinItem *)(base + l.qs);
   a.qb = (MinItem *)(base + l.qb);
   a.cap_s = l.cap_s;

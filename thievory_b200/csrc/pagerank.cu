@@ -43,7 +43,8 @@ struct PrArgs {
   const uint32_t *split_parts;
   double *dang;
   uint32_t *tile_ctr;
-  uint32_t ntiles, nv, it, pad;
+  uint32_t ntiles, nv, it;
+  uint32_t wshift;  // packed weighted edges: the id is e >> wshift
   double damping, inv_n;
 };
 
@@ -78,8 +79,8 @@ __device__ __forceinline__ double finish_vertex(const PrArgs &a, uint32_t v,
 }
 
 template <int ESZ>
-__device__ __forceinline__ uint32_t staged_id(const uint32_t *s_e, uint32_t i) {
-  return s_e[(size_t)i * (ESZ / 4)];
+__device__ __forceinline__ uint32_t staged_id(const uint32_t *s_e, uint32_t i, uint32_t wshift) {
+  return ESZ == 4 ? edge_dst(s_e[i], wshift) : s_e[(size_t)i * 2];
 }
 
 // Stage edges [t.ebegin, t.eend) of a tile; returns the element shift.
@@ -131,7 +132,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_pull_kernel(PrArgs a) {
       const uint32_t cnt = (uint32_t)(t.eend - t.ebegin);
       double part = 0.0;
       for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
-        part += (double)__ldg(a.cur + staged_id<ESZ>(s_e, shift + i));
+        part += (double)__ldg(a.cur + staged_id<ESZ>(s_e, shift + i, a.wshift));
       part = block_sum(part, s_red);
       if (threadIdx.x == 0) {
         const uint32_t s = t.split - 1;
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_pull_kernel(PrArgs a) {
           double x = 0.0;
           int pos = 32;
           if (tt < total) {
-            x = (double)__ldg(a.cur + staged_id<ESZ>(s_e, shift + ols + (tt - oex)));
+            x = (double)__ldg(a.cur + staged_id<ESZ>(s_e, shift + ols + (tt - oex), a.wshift));
             pos = o;
           }
 #pragma unroll
@@ -211,7 +212,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_push_kernel(PrArgs a) {
       const double c = (double)__ldg(a.cur + t.vbegin);
       const uint32_t cnt = (uint32_t)(t.eend - t.ebegin);
       for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
-        atomicAdd(a.sum + staged_id<ESZ>(s_e, shift + i), c);
+        atomicAdd(a.sum + staged_id<ESZ>(s_e, shift + i, a.wshift), c);
     } else {
       const uint32_t nverts = t.vend - t.vbegin;
       const uint32_t ngroups = (nverts + 31) / 32;
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_push_kernel(PrArgs a) {
           const unsigned oex = __shfl_sync(kFull, excl, o);
           const float oc = __shfl_sync(kFull, c, o);
           if (tt < total)
-            atomicAdd(a.sum + staged_id<ESZ>(s_e, shift + ols + (tt - oex)), (double)oc);
+            atomicAdd(a.sum + staged_id<ESZ>(s_e, shift + ols + (tt - oex), a.wshift), (double)oc);
         }
       }
     }
@@ -372,6 +373,7 @@ thv_status run_pagerank(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.nv = (uint32_t)g->nv;
   a.damping = damping;
   a.inv_n = 1.0 / (double)g->nv;
+  a.wshift = g->wshift;
 
   uint32_t launches = 0;
   THV_CUDA(cudaEventRecord(p->ev0, st));

@@ -54,6 +54,7 @@ struct SvArgs {
   const uint32_t *blk_vb;
   const uint64_t *blk_base;
   uint64_t host_base;
+  ListCache lc;
   uint32_t *val;  // [nv][W]
   unsigned long long *front;
   uint32_t *bm;
@@ -64,7 +65,9 @@ struct SvArgs {
   unsigned long long active, unit;
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, W;
-  uint32_t max_iters, small_deg, chunk, pad;
+  uint32_t max_iters, small_deg, chunk;
+  uint32_t wshift, wbase;  // 4-byte edges: see edge_dst / edge_wt
+  uint32_t pad;
 };
 
 __device__ __forceinline__ unsigned long long warp_or(unsigned long long x) {
@@ -113,7 +116,9 @@ __device__ __forceinline__ void sv_item_rows(const SvArgs &a, uint32_t u, uintpt
     uint32_t ex = 0, ey = 1;
     if (k < cnt) {
       if (ESZ == 4) {
-        ex = ld_nc_u32(eaddr + (uintptr_t)k * 4u);
+        const uint32_t r = ld_nc_u32(eaddr + (uintptr_t)k * 4u);
+        ex = edge_dst(r, a.wshift);
+        ey = edge_wt(r, a.wshift, a.wbase);
       } else {
         const uint2 e = ld_nc_u2(eaddr + (uintptr_t)k * 8u);
         ex = e.x;
@@ -171,7 +176,8 @@ __device__ __forceinline__ void sv_chunk(const SvArgs &a, const WorkItem &it, un
     for (int j = 0; j < PER; j++) {
       const uintptr_t ea = p + (uintptr_t)ESZ * j;
       if (ea >= start && ea < end)
-        sv_edge(a, it.v, ESZ == 4 ? e[j] : e[2 * j], ESZ == 4 ? 1u : e[2 * j + 1], f);
+        sv_edge(a, it.v, ESZ == 4 ? edge_dst(e[j], a.wshift) : e[2 * j],
+                ESZ == 4 ? edge_wt(e[j], a.wshift, a.wbase) : e[2 * j + 1], f);
     }
   }
 }
@@ -211,7 +217,8 @@ __device__ __forceinline__ void sv_group(const SvArgs &a, unsigned long long fir
     if (t < total) {
       const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
       if (ESZ == 4) {
-        sv_edge(a, ou, ld_nc_u32(addr), 1u, of);
+        const uint32_t r = ld_nc_u32(addr);
+        sv_edge(a, ou, edge_dst(r, a.wshift), edge_wt(r, a.wshift, a.wbase), of);
       } else {
         const uint2 e = ld_nc_u2(addr);
         sv_edge(a, ou, e.x, e.y, of);
@@ -284,11 +291,12 @@ __global__ void __launch_bounds__(kSvThreads) sv_kernel(SvArgs a) {
         if (take) {
           const uint64_t s0 = __ldg(a.off + v), e0 = __ldg(a.off + v + 1);
           deg = (uint32_t)(e0 - s0);
-          const unsigned long long base = __ldg(a.blk_base + find_block(vb, a.nblk, v));
-          eaddr = base + s0 * ESZ;
+          bool host;
+          eaddr = list_addr(a.lc, __ldg(a.blk_base + find_block(vb, a.nblk, v)), a.host_base, v,
+                            s0, deg, ESZ, &host);
           my_edges += deg;
           my_pairs += __popcll(take);
-          if (base == a.host_base) my_link += (unsigned long long)deg * ESZ;
+          if (host) my_link += (unsigned long long)deg * ESZ;
           else my_hbm += (unsigned long long)deg * ESZ;
         }
         const bool small = take && deg > 0 && deg < a.small_deg;
@@ -530,6 +538,10 @@ SvArgs make_args(thv_server *s) {
   a.blk_vb = g->plan.d_vbegin;
   a.blk_base = g->plan.d_base;
   a.host_base = g->h_edges_dev;
+  a.lc = list_cache_of(g->plan);
+  // 4-byte edges: packed weights, or unit weights for an unweighted graph
+  a.wshift = g->wshift;
+  a.wbase = g->packed ? g->wbase : 1u;
   a.val = s->d_val;
   a.front = s->d_front;
   a.bm = s->d_bm;

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "thv_internal.h"
+
 namespace thv {
 
 constexpr unsigned kFull = 0xFFFFFFFFu;
@@ -109,6 +111,29 @@ __device__ __forceinline__ uint32_t find_block(const uint32_t *vb, uint32_t nblk
     else hi = mid;
   }
   return lo;
+}
+
+// A 4-byte edge: the neighbour id in the high bits and, for packed weighted
+// graphs, w - wbase in the low wshift bits (wshift = 0: an id-only edge).
+__device__ __forceinline__ uint32_t edge_dst(uint32_t e, uint32_t wshift) { return e >> wshift; }
+__device__ __forceinline__ uint32_t edge_wt(uint32_t e, uint32_t wshift, uint32_t wbase) {
+  return (e & ((1u << wshift) - 1u)) + wbase;
+}
+
+// Device address of the first edge of v's list, given its block's base and
+// its first edge index s0; *host says whether it is read over the host link.
+__device__ __forceinline__ unsigned long long list_addr(const ListCache &lc,
+                                                       unsigned long long block_base,
+                                                       unsigned long long host_base, uint32_t v,
+                                                       uint64_t s0, uint32_t deg, uint32_t esz,
+                                                       bool *host) {
+  const bool on_host = block_base == host_base;
+  if (on_host && deg < lc.deg_lt && deg > 0) {
+    *host = false;
+    return lc.base + (unsigned long long)__ldg(lc.idx + v) * esz;
+  }
+  *host = on_host;
+  return block_base + s0 * esz;
 }
 
 // Grid-wide barrier for a cooperative launch.  The wait is bounded by

@@ -52,6 +52,11 @@ struct __align__(16) PrTile {
   uint32_t split;  // 0, or 1 + index of the split vertex
 };
 
+constexpr uint64_t kDefaultBlockBytes = 64ull << 20;  // reference PARTITION_SIZE_MB
+constexpr size_t kEdgePad = 1024;                     // bytes of slack past arrays
+constexpr uint32_t kDefaultListDeg = 64;  // small-list cache threshold (CSR/WCSR)
+constexpr size_t kListLead = 128;         // slack before the first cached list
+
 struct Plan {
   bool valid = false;
   uint64_t budget_bytes = 0, block_bytes = 0;
@@ -64,6 +69,13 @@ struct Plan {
   uint32_t *d_vbegin = nullptr;
   uint64_t *d_base = nullptr;
   uint64_t resident_edge_bytes = 0, host_edge_bytes = 0;
+  // small-list cache: lists with 0 < deg < list_deg in host blocks, packed
+  // in d_lists (element 0 at d_lists + kListLead); d_list_idx[v] = element
+  // index of v's list
+  uint32_t list_deg = 0;
+  char *d_lists = nullptr;
+  uint32_t *d_list_idx = nullptr;
+  uint64_t list_bytes = 0, list_vertices = 0, d_lists_bytes = 0;
   // PageRank tiles (built lazily)
   bool tiles_valid = false;
   std::vector<PrTile> tiles;
@@ -72,6 +84,25 @@ struct Plan {
   uint32_t *d_split_parts = nullptr;
   uint64_t tiles_hbm_bytes = 0, tiles_link_bytes = 0;
 };
+
+// Small-list cache as the kernels see it: lists with 0 < deg < deg_lt whose
+// block is read from the host are mirrored in HBM; idx[v] is the element
+// index of v's list there (element 0 at base).  deg_lt = 0 disables it.
+struct ListCache {
+  const uint32_t *idx;
+  unsigned long long base;
+  uint32_t deg_lt, pad;
+};
+
+inline ListCache list_cache_of(const Plan &p) {
+  ListCache c{nullptr, 0, 0, 0};
+  if (p.list_deg && p.d_lists) {
+    c.idx = p.d_list_idx;
+    c.base = (unsigned long long)(p.d_lists + kListLead);
+    c.deg_lt = p.list_deg;
+  }
+  return c;
+}
 
 struct MinState;  // minprop.cu
 struct PrState;   // pagerank.cu
@@ -82,8 +113,11 @@ struct BatchState;  // batch.cu
 struct thv_graph {
   uint64_t nv = 0, ne = 0;
   thv_format fmt = THV_FMT_CSR;
-  uint32_t esz = 4;
+  uint32_t esz = 4;       // bytes per edge in memory (host and HBM copies)
   bool weighted = false;
+  // packed weighted edges: 4 bytes = dst << wshift | (w - wbase)
+  bool packed = false;
+  uint32_t wshift = 0, wbase = 0;
   int device = 0;
   // host
   std::vector<uint64_t> off;      // nv+1
@@ -91,6 +125,7 @@ struct thv_graph {
   size_t h_edges_bytes = 0;
   uint64_t h_edges_dev = 0;       // device address of h_edges
   std::vector<uint32_t> outdeg;   // CSC only
+  mutable std::vector<uint32_t> h_unpacked;  // {dst, w} view of packed edges
   // device
   cudaStream_t stream = nullptr;
   uint64_t *d_off = nullptr;
@@ -107,10 +142,9 @@ struct thv_graph {
 
 namespace thv {
 
-constexpr uint64_t kDefaultBlockBytes = 64ull << 20;  // reference PARTITION_SIZE_MB
-constexpr size_t kEdgePad = 1024;                     // bytes of slack past arrays
 
 thv_status graph_init_device(thv_graph *g);  // stream, d_off, d_outdeg
+thv_status set_packing(thv_graph *g, bool on);  // weighted graphs only
 thv_status ensure_plan(thv_graph *g);
 thv_status build_tiles(thv_graph *g);
 void plan_free(thv_graph *g);
