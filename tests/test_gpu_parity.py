@@ -91,6 +91,18 @@ def test_sssp_delta_independent(T, O, g14w, delta):
         assert np.array_equal(got, O.sssp(g14w, src))
 
 
+@pytest.mark.parametrize("growth", [1, 2, 8, 1 << 20])
+@pytest.mark.parametrize("mode", ["scan", "queue"])
+def test_sssp_growth_independent(T, O, g14w, growth, mode):
+    src = int(O.sources(g14w, 1)[0])
+    with engine_graph(T, g14w, "wcsr") as g:
+        plan(g, 0.4)
+        for delta in (1, 8):
+            got, _ = g.run("sssp", source=src, sssp_delta=delta, sssp_growth=growth,
+                           compaction=mode, timeout_ms=20000)
+            assert np.array_equal(got, O.sssp(g14w, src)), (delta, growth, mode)
+
+
 @pytest.mark.parametrize("small,chunk", [(1, 32), (32, 64), (1024, 1024)])
 def test_expansion_tuning_is_result_neutral(T, O, g14, small, chunk):
     with engine_graph(T, g14) as g:

@@ -49,7 +49,7 @@ class _RunOpts(ctypes.Structure):
                 ("pr_damping", ctypes.c_double), ("sssp_delta", ctypes.c_uint32),
                 ("timeout_ms", ctypes.c_uint32), ("stream", ctypes.c_void_p),
                 ("small_degree", ctypes.c_uint32), ("chunk_edges", ctypes.c_uint32),
-                ("flags", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+                ("flags", ctypes.c_uint32), ("sssp_growth", ctypes.c_uint32)]
 
 
 class _Stats(ctypes.Structure):
@@ -280,15 +280,17 @@ class Graph:
     def run(self, algo: str, source: int = 1, pr_iters: int = 20, pr_damping: float = 0.85,
             out: Optional[np.ndarray] = None, want_values: bool = True, stream: int = 0,
             sssp_delta: int = 0, timeout_ms: int = 0, small_degree: int = 0,
-            chunk_edges: int = 0, checksum: bool = False, compaction: str = ""):
+            chunk_edges: int = 0, checksum: bool = False, compaction: str = "",
+            sssp_growth: int = 0):
         """Run algo; returns (values or None, stats dict).  compaction:
-        "" (per-algorithm default), "scan" or "queue"."""
+        "" (per-algorithm default), "scan" or "queue"; sssp_growth: SSSP
+        window growth per advance (0 = default 8, 1 = fixed windows)."""
         lib = load_library()
         flags = ((1 if checksum else 0) | (2 if compaction == "scan" else 0)
                  | (4 if compaction == "queue" else 0))
         o = _RunOpts(source, pr_iters, pr_damping, sssp_delta, timeout_ms,
                      ctypes.c_void_p(stream) if stream else None, small_degree, chunk_edges,
-                     flags, 0)
+                     flags, sssp_growth)
         st = _Stats()
         buf = None
         if want_values:
