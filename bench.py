@@ -39,12 +39,14 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 # DRAM and host-link (sysmem) bytes per launch of the dominant kernel, from the
-# ncu captures summarised in profiles/ (minprop_sssp_rmat22_wcsr_hbm40.md,
-# minprop_bfs_rmat20_resident.md, pr_pull_rmat22_csc_hbm47.md).  Captures
+# ncu captures summarised in profiles/ (minq_sssp_rmat22_wcsr_packed_hbm40.md,
+# minprop_cc_rmat22_sym_hbm40.md, minprop_bfs_rmat20_resident.md,
+# pr_pull_rmat22_csc_hbm47.md).  Captures
 # made on a smaller graph are scaled to the bench size by edge count (the
 # traffic of these kernels grows with the edges traversed).
 NCU_TRAFFIC = {
-    "sssp": dict(scale=22, ne=65241959, dram=298979072 + 14398464, sysmem=11397242 * 32),
+    "sssp": dict(scale=22, ne=65241959, dram=600403968 + 87389440, sysmem=3375952 * 32),
+    "cc": dict(scale=22, ne=128306542, dram=392704512 + 69563648, sysmem=11788847 * 32),
     "bfs": dict(scale=20, ne=16084564, dram=78297088 + 4716544, sysmem=0),
     "pr_pull": dict(scale=22, ne=65241959, dram=135399168 + 20317184, sysmem=6104134 * 32, per="iteration"),
 }
