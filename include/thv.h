@@ -223,6 +223,7 @@ typedef struct thv_batch_opts {
                             configuration and keep the fastest (cached per
                             graph shape in memory and in $THV_TUNE_CACHE or
                             ~/.cache/thievory_b200_batch_tune.txt) */
+  uint32_t sssp_growth;  /* SSSP window width factor per advance; 0 = default */
 } thv_batch_opts;
 
 /* Runs n sources in groups sharing one traversal each.  out (host, may be

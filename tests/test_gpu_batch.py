@@ -50,6 +50,24 @@ def test_batched_sssp_equals_single(T, O, g14w, frac):
             assert int(sums[i]) == T.values_checksum(want)
 
 
+def test_sssp_window_options_reach_the_kernel(T, O, g14w):
+    """Each call's window and growth must be used even when the launch
+    sequence was captured by an earlier call with other options."""
+    src = sources(O, g14w, 64)
+    with T.Graph.from_arrays(g14w.off, g14w.wcsr_edges(), "wcsr") as g:
+        g.plan(int(0.4 * g.ne * 8), block_bytes=BLOCK)
+        iters = {}
+        ref = None
+        for delta, growth in [(64, 1), (1, 1), (64, 1), (1, 8), (4, 2)]:
+            _, sums, st = g.batch_run("sssp", src, sssp_delta=delta, sssp_growth=growth,
+                                      want_values=False, timeout_ms=20000)
+            if ref is None:
+                ref = sums
+            assert np.array_equal(sums, ref), (delta, growth)
+            iters[(delta, growth)] = st["iterations"]
+        assert iters[(1, 1)] > iters[(1, 8)] and iters[(1, 1)] > iters[(64, 1)]
+
+
 def test_batched_checksums_only(T, O, g14w):
     src = sources(O, g14w, 64)
     with T.Graph.from_arrays(g14w.off, g14w.wcsr_edges(), "wcsr") as g:

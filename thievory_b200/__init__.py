@@ -93,7 +93,7 @@ class _BatchOpts(ctypes.Structure):
     _fields_ = [("group", ctypes.c_uint32), ("timeout_ms", ctypes.c_uint32),
                 ("stream", ctypes.c_void_p), ("small_degree", ctypes.c_uint32),
                 ("chunk_edges", ctypes.c_uint32), ("sssp_delta", ctypes.c_uint32),
-                ("tune", ctypes.c_uint32)]
+                ("tune", ctypes.c_uint32), ("sssp_growth", ctypes.c_uint32)]
 
 
 class _ServeOpts(ctypes.Structure):
@@ -307,14 +307,14 @@ class Graph:
     def batch_run(self, algo: str, sources: Sequence[int], group: int = 64,
                   want_values: bool = True, stream: int = 0, small_degree: int = 0,
                   chunk_edges: int = 0, timeout_ms: int = 0, sssp_delta: int = 0,
-                  tune: bool = False):
+                  tune: bool = False, sssp_growth: int = 0):
         """Batched BFS/SSSP; returns (values [n, nv] or None, checksums [n], stats)."""
         lib = load_library()
         src = np.ascontiguousarray(sources, dtype=np.uint32)
         out = np.empty((len(src), self.nv), dtype=np.uint32) if want_values else None
         sums = np.empty(len(src), dtype=np.uint64)
         o = _BatchOpts(group, timeout_ms, ctypes.c_void_p(stream) if stream else None,
-                       small_degree, chunk_edges, sssp_delta, 1 if tune else 0)
+                       small_degree, chunk_edges, sssp_delta, 1 if tune else 0, sssp_growth)
         st = _Stats()
         _check(lib.thv_batch_run(self._h, ALGO[algo], _ptr(src), len(src), ctypes.byref(o),
                                  None if out is None else _ptr(out), _ptr(sums),

@@ -36,6 +36,7 @@ namespace thv {
 enum { MS_BFS = 0, MS_SSSP = 1 };
 constexpr uint32_t kMsWidth = 64;       // sources per group (mask bits)
 constexpr uint32_t kMaxBfsLevel = 254;  // u8 level bytes hold level + 1
+constexpr uint32_t kMsGrowth = 1;       // SSSP window width factor per advance
 
 struct MsCtrl {
   GridBar bar;
@@ -66,7 +67,7 @@ struct MsArgs {
   uint32_t nblk, nv, ngroups, max_iters;
   uint32_t small_deg, chunk, delta;
   uint32_t wshift, wbase;  // packed weighted edges (see edge_dst / edge_wt)
-  uint32_t pad;
+  uint32_t growth;         // SSSP window width factor per advance
 };
 
 struct BatchState {
@@ -300,6 +301,7 @@ __global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
   const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
   const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
   uint32_t thr = OP == MS_SSSP ? (uint32_t)min(1ull + a.delta, 0xFFFFFFFFull) : 0xFFFFFFFFu;
+  uint32_t width = a.delta;
   unsigned iter = 0, level = 1;  // BFS level of the vertices being expanded
   for (;; ++iter) {
     if (iter >= a.max_iters || (OP == MS_BFS && level > kMaxBfsLevel)) {
@@ -342,14 +344,25 @@ __global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
           if (OP == MS_BFS) {
             take = f;
           } else {
+            // the pending sources' distances, eight loads in flight
             const uint32_t *dv = a.dist + (size_t)v * kMsWidth;
             unsigned long long r = f;
             while (r) {
-              const int s = __ffsll((long long)r) - 1;
-              r &= r - 1;
-              const uint32_t d = ldcg(dv + s);
-              if (d < thr) take |= 1ull << s;
-              else kmin = min(kmin, d);
+              int s[8];
+              uint32_t d[8];
+#pragma unroll
+              for (int k = 0; k < 8; k++) {
+                s[k] = r ? __ffsll((long long)r) - 1 : -1;
+                r &= r - 1;
+              }
+#pragma unroll
+              for (int k = 0; k < 8; k++) d[k] = s[k] >= 0 ? ldcg(dv + s[k]) : 0u;
+#pragma unroll
+              for (int k = 0; k < 8; k++) {
+                if (s[k] < 0) continue;
+                if (d[k] < thr) take |= 1ull << s[k];
+                else kmin = min(kmin, d[k]);
+              }
             }
             keep = f & ~take;
           }
@@ -443,7 +456,8 @@ __global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
     if (ns + nb == 0) {
       if (OP == MS_BFS) break;
       if (ldcg(&c->remaining[slot]) == 0) break;
-      thr = (uint32_t)min((unsigned long long)ldcg(&c->minkept[slot]) + a.delta, 0xFFFFFFFFull);
+      width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
+      thr = (uint32_t)min((unsigned long long)ldcg(&c->minkept[slot]) + width, 0xFFFFFFFFull);
       continue;
     }
     // ----------------------------------------------------------- expansion
@@ -579,13 +593,17 @@ const MsConfig kMsCandidates[] = {{16, 128, 512}, {64, 256, 512}, {256, 512, 512
                                   {256, 512, 256}, {64, 1024, 256}};
 constexpr uint32_t kMsMinSmall = 16, kMsMinChunk = 128;
 
+// A captured launch sequence holds its kernel arguments by value, so the key
+// covers every argument that can differ between calls on one batch state.
 struct GraphKey {
   int op, esz, threads;
   bool out;
-  uint32_t small, chunk;
+  uint32_t small, chunk, delta, growth;
+  unsigned long long timeout_ns;
   bool operator<(const GraphKey &o) const {
-    return std::tie(op, esz, threads, out, small, chunk) <
-           std::tie(o.op, o.esz, o.threads, o.out, o.small, o.chunk);
+    return std::tie(op, esz, threads, out, small, chunk, delta, growth, timeout_ns) <
+           std::tie(o.op, o.esz, o.threads, o.out, o.small, o.chunk, o.delta, o.growth,
+                    o.timeout_ns);
   }
 };
 
@@ -718,7 +736,8 @@ static thv_status run_group(thv_graph *g, bool sssp, MsArgs &a, cudaStream_t st,
                             const MsConfig &cfg, uint32_t &launches) {
   BatchState *b = g->bs;
   BatchExtra &ex = g_extra[b];
-  const GraphKey key{sssp ? 1 : 0, (int)g->esz, (int)cfg.threads, want_out, cfg.small, cfg.chunk};
+  const GraphKey key{sssp ? 1 : 0, (int)g->esz, (int)cfg.threads, want_out, cfg.small, cfg.chunk,
+                     a.delta,     a.growth,    a.timeout_ns};
   auto it = ex.graphs.find(key);
   if (it == ex.graphs.end() && ex.capture_ok) {
     cudaStream_t cs = nullptr;
@@ -881,6 +900,7 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
   // 64: many sources expand a vertex in the same iteration and share its
   // adjacency read (small windows make each source re-read it)
   a.delta = o && o->sssp_delta ? o->sssp_delta : 64u;
+  a.growth = o && o->sssp_growth ? o->sssp_growth : kMsGrowth;
 
   thv_stats local{};
   uint32_t launches = 0;
