@@ -217,7 +217,7 @@ typedef struct thv_batch_opts {
   void *stream;
   uint32_t small_degree; /* expansion tuning; 0 = autotuned / default */
   uint32_t chunk_edges;  /* expansion tuning; 0 = autotuned / default */
-  uint32_t sssp_delta;   /* shared near/far width for SSSP; 0 = 64 */
+  uint32_t sssp_delta;   /* shared near/far width for SSSP; 0 = 256 */
   uint32_t tune;         /* 1: without small_degree/chunk_edges, time the
                             first group under each candidate launch
                             configuration and keep the fastest (cached per
@@ -251,6 +251,11 @@ typedef struct thv_serve_opts {
   uint32_t timeout_ms;       /* bound on device waits; 0 = 60000 */
   uint32_t max_batch_iters;  /* iterations per launch while requests wait;
                                 0 = 4 */
+  uint32_t group_min;        /* queue depth from which waiting queries run
+                                as batched groups of up to 64 (the
+                                thv_batch_run kernels) instead of slots;
+                                0 = 2, 0xFFFFFFFF = never (slots only) */
+  uint32_t pad;
 } thv_serve_opts;
 
 typedef struct thv_query_stats {
@@ -261,7 +266,9 @@ typedef struct thv_query_stats {
   uint32_t iterations;
   uint32_t slot;
   int32_t status;    /* thv_status of the query */
-  uint32_t pad;
+  uint32_t grouped;  /* 0: ran in a slot; 1: in a batched group (slot =
+                        position in it); 2: alone on the single-source
+                        kernel (the server was idle) */
 } thv_query_stats;
 
 thv_status thv_serve_start(thv_graph *g, const thv_serve_opts *o,

@@ -42,7 +42,8 @@ def test_serve_mixed_stream(T, O, g14w, eg):
 
 def test_serve_arrivals_join_running_traversal(T, O, g14w, eg):
     src = O.sources(g14w, 24).tolist()
-    with T.Server(eg, max_slots=4, max_batch_iters=1, timeout_ms=20000) as sv:
+    with T.Server(eg, max_slots=4, max_batch_iters=1, group_min=0xFFFFFFFF,
+                  timeout_ms=20000) as sv:
         tickets = []
         for i, s in enumerate(src):
             tickets.append((sv.submit("sssp" if i % 3 == 0 else "bfs", s), s, i))
@@ -59,7 +60,7 @@ def test_serve_same_result_alone_and_in_mix(T, O, g14w, eg):
     s0 = int(O.sources(g14w, 1)[0])
     with T.Server(eg, max_slots=1) as sv:
         alone, st_a = sv.wait(sv.submit("sssp", s0))
-    with T.Server(eg, max_slots=16) as sv:
+    with T.Server(eg, max_slots=16, group_min=0xFFFFFFFF) as sv:
         ts = [sv.submit("bfs", s) for s in O.sources(g14w, 10)]
         t0 = sv.submit("sssp", s0)
         ts += [sv.submit("bfs", s) for s in O.sources(g14w, 20)[10:]]
@@ -109,3 +110,55 @@ def test_serve_rejects_bad_requests(T, O, g14w, eg):
         with pytest.raises(T.ThvError):
             sv.submit("sssp", 1)
     gu.close()
+
+
+def test_deep_queue_runs_as_batched_groups(T, O, g14w, eg):
+    src = O.sources(g14w, 100).tolist()
+    algos = ["sssp" if i % 4 == 0 else "bfs" for i in range(len(src))]
+    with T.Server(eg, max_slots=8, group_min=16, timeout_ms=20000) as sv:
+        tickets = [sv.submit(a, s, want_values=(i % 2 == 0)) for i, (a, s) in
+                   enumerate(zip(algos, src))]
+        grouped = 0
+        for i, (t, a, s) in enumerate(zip(tickets, algos, src)):
+            vals, st = sv.wait(t)
+            w = want(O, g14w, a, s)
+            assert st["checksum"] == T.values_checksum(w), f"{a} {s}"
+            if i % 2 == 0:
+                assert np.array_equal(vals, w), f"{a} {s}"
+            grouped += st["grouped"]
+        assert grouped > 0
+
+
+def test_group_mode_can_be_switched_off(T, O, g14w, eg):
+    src = O.sources(g14w, 60).tolist()
+    with T.Server(eg, max_slots=4, group_min=0xFFFFFFFF, timeout_ms=20000) as sv:
+        tickets = [(sv.submit("bfs", s), s) for s in src]
+        for t, s in tickets:
+            vals, st = sv.wait(t)
+            assert st["grouped"] != 1 and st["slot"] < 4
+            assert np.array_equal(vals, O.bfs(g14w, s))
+
+
+def test_idle_server_runs_a_lone_query_on_the_single_source_kernel(T, O, g14w, eg):
+    s0 = int(O.sources(g14w, 1)[0])
+    with T.Server(eg, max_slots=8, timeout_ms=20000) as sv:
+        for algo in ("bfs", "sssp"):
+            vals, st = sv.wait(sv.submit(algo, s0))
+            assert st["grouped"] == 2
+            assert np.array_equal(vals, want(O, g14w, algo, s0))
+            assert st["checksum"] == T.values_checksum(vals)
+
+
+@pytest.mark.parametrize("group_min", [0, 16, 0xFFFFFFFF])
+def test_all_serving_modes_agree(T, O, g14w, eg, group_min):
+    src = O.sources(g14w, 40).tolist()
+    algos = ["sssp" if i % 3 == 0 else "bfs" for i in range(len(src))]
+    with T.Server(eg, max_slots=8, group_min=group_min, timeout_ms=20000) as sv:
+        tickets = [sv.submit(a, s, want_values=False) for a, s in zip(algos, src)]
+        modes = set()
+        for t, a, s in zip(tickets, algos, src):
+            _, st = sv.wait(t)
+            modes.add(st["grouped"])
+            assert st["checksum"] == T.values_checksum(want(O, g14w, a, s)), (a, s)
+        if group_min == 0xFFFFFFFF:
+            assert 1 not in modes

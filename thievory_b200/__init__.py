@@ -99,14 +99,15 @@ class _BatchOpts(ctypes.Structure):
 class _ServeOpts(ctypes.Structure):
     _fields_ = [("max_slots", ctypes.c_uint32), ("queue_capacity", ctypes.c_uint32),
                 ("mem_budget_bytes", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32),
-                ("max_batch_iters", ctypes.c_uint32)]
+                ("max_batch_iters", ctypes.c_uint32), ("group_min", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32)]
 
 
 class _QueryStats(ctypes.Structure):
     _fields_ = [("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
                 ("latency_ms", ctypes.c_double), ("checksum", ctypes.c_uint64),
                 ("iterations", ctypes.c_uint32), ("slot", ctypes.c_uint32),
-                ("status", ctypes.c_int32), ("pad", ctypes.c_uint32)]
+                ("status", ctypes.c_int32), ("grouped", ctypes.c_uint32)]
 
     def to_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
@@ -371,11 +372,15 @@ class Server:
     (kept alive here until the ticket completes)."""
 
     def __init__(self, graph: Graph, max_slots: int = 64, queue_capacity: int = 0,
-                 mem_budget_bytes: int = 0, timeout_ms: int = 0, max_batch_iters: int = 0):
+                 mem_budget_bytes: int = 0, timeout_ms: int = 0, max_batch_iters: int = 0,
+                 group_min: int = 0):
+        """group_min: queue depth from which waiting queries run as batched
+        groups (0 = 2, 0xFFFFFFFF = never: slots only)."""
         lib = load_library()
         self.graph = graph
         self._bufs = {}
-        o = _ServeOpts(max_slots, queue_capacity, mem_budget_bytes, timeout_ms, max_batch_iters)
+        o = _ServeOpts(max_slots, queue_capacity, mem_budget_bytes, timeout_ms, max_batch_iters,
+                       group_min, 0)
         self._h = ctypes.c_void_p()
         _check(lib.thv_serve_start(graph._h, ctypes.byref(o), ctypes.byref(self._h)),
                "thv_serve_start")

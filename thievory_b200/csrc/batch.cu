@@ -37,6 +37,7 @@ enum { MS_BFS = 0, MS_SSSP = 1 };
 constexpr uint32_t kMsWidth = 64;       // sources per group (mask bits)
 constexpr uint32_t kMaxBfsLevel = 254;  // u8 level bytes hold level + 1
 constexpr uint32_t kMsGrowth = 1;       // SSSP window width factor per advance
+constexpr uint32_t kMsDelta = 256;      // SSSP window width shared by a group
 
 struct MsCtrl {
   GridBar bar;
@@ -73,6 +74,7 @@ struct MsArgs {
 struct BatchState {
   uint64_t nv = 0;
   bool sssp = false;
+  bool valid = false;  // every allocation succeeded
   unsigned long long *d_visit = nullptr, *d_front = nullptr;
   uint8_t *d_lvl = nullptr;
   uint32_t *d_dist = nullptr;
@@ -616,8 +618,7 @@ static std::map<BatchState *, BatchExtra> g_extra;  // graphs per batch state
 static std::mutex g_tune_mu;
 static std::map<std::string, MsConfig> g_tune;     // in-process tuner cache
 
-void batch_free(thv_graph *g) {
-  BatchState *b = g->bs;
+static void free_state(BatchState *&b) {
   if (!b) return;
   auto it = g_extra.find(b);
   if (it != g_extra.end()) {
@@ -644,16 +645,29 @@ void batch_free(thv_graph *g) {
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   delete b;
+  b = nullptr;
+}
+
+void batch_free(thv_graph *g) {
+  free_state(g->bs_keep[0]);
+  free_state(g->bs_keep[1]);
   g->bs = nullptr;
 }
 
 // Queues are sized for the smallest bucket boundary and chunk any
-// configuration may use, so tuning never reallocates.
+// configuration may use, so tuning never reallocates.  BFS and SSSP keep
+// separate states, so alternating between them (served groups) does not
+// reallocate either.
 static thv_status ensure_batch_state(thv_graph *g, bool sssp, bool want_out) {
-  BatchState *&b = g->bs;
-  if (b && b->sssp == sssp && (!want_out || b->d_out)) return THV_OK;
-  batch_free(g);
+  BatchState *&b = g->bs_keep[sssp ? 1 : 0];
+  g->bs = nullptr;
+  if (b && b->valid && (!want_out || b->d_out)) {
+    g->bs = b;
+    return THV_OK;
+  }
+  free_state(b);
   b = new BatchState();
+  g->bs = b;
   b->nv = g->nv;
   b->sssp = sssp;
   const uint64_t nw = (g->nv + 31) / 32;
@@ -683,6 +697,7 @@ static thv_status ensure_batch_state(thv_graph *g, bool sssp, bool want_out) {
   if (want_out) THV_TRY(dev_alloc((void **)&b->d_out, (uint64_t)kMsWidth * g->nv * 4 + 64, "batch output"));
   THV_CUDA(cudaEventCreate(&b->ev0));
   THV_CUDA(cudaEventCreate(&b->ev1));
+  b->valid = true;
   return THV_OK;
 }
 
@@ -773,7 +788,7 @@ static unsigned long long host_value_hash(uint32_t v, uint32_t val) {
 }
 
 static thv_status fallback_single(thv_graph *g, const uint32_t *src, uint32_t k, cudaStream_t st,
-                                  const thv_batch_opts *o, uint32_t *out, uint64_t *sums,
+                                  const thv_batch_opts *o, uint32_t *const *rows, uint64_t *sums,
                                   thv_stats &acc) {
   std::vector<uint32_t> vals(g->nv);
   for (uint32_t i = 0; i < k; i++) {
@@ -782,7 +797,7 @@ static thv_status fallback_single(thv_graph *g, const uint32_t *src, uint32_t k,
     ro.timeout_ms = o ? o->timeout_ms : 0;
     thv_stats st1{};
     THV_TRY(run_minprop(g, THV_ALGO_BFS, &ro, st, &st1));
-    uint32_t *dst = out ? out + (uint64_t)i * g->nv : vals.data();
+    uint32_t *dst = rows && rows[i] ? rows[i] : vals.data();
     THV_TRY(minprop_values(g, dst, st));
     if (sums) {
       unsigned long long h = 0;
@@ -855,6 +870,21 @@ static void tune_store(const std::string &key, const MsConfig &c) {
 thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
                      uint32_t n, const thv_batch_opts *o, uint32_t *out,
                      uint64_t *checksums, thv_stats *stats) {
+  std::vector<uint32_t *> rows;
+  if (out) {
+    rows.resize(n);
+    for (uint32_t i = 0; i < n; i++) rows[i] = out + (uint64_t)i * g->nv;
+  }
+  return run_batch_rows(g, algo, sources, n, o, out ? rows.data() : nullptr, checksums, stats);
+}
+
+// As run_batch, with one destination per source (rows[i] may be null; rows
+// may be null for checksums only).
+thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
+                          uint32_t n, const thv_batch_opts *o, uint32_t *const *rows,
+                          uint64_t *checksums, thv_stats *stats) {
+  bool want_out = false;
+  for (uint32_t i = 0; rows && i < n; i++) want_out |= rows[i] != nullptr;
   if (algo != THV_ALGO_BFS && algo != THV_ALGO_SSSP)
     return fail(THV_EINVAL, "batched runs support BFS and SSSP");
   const bool sssp = algo == THV_ALGO_SSSP;
@@ -866,7 +896,7 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
   const uint32_t group = o && o->group ? std::min<uint32_t>(o->group, kMsWidth) : kMsWidth;
   const double t0 = now_ms();
   THV_TRY(ensure_plan(g));
-  THV_TRY(ensure_batch_state(g, sssp, out != nullptr));
+  THV_TRY(ensure_batch_state(g, sssp, want_out));
   BatchState *b = g->bs;
   cudaStream_t st = o && o->stream ? (cudaStream_t)o->stream : g->stream;
   MsArgs a{};
@@ -897,9 +927,11 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
   a.nv = (uint32_t)g->nv;
   a.ngroups = b->ngroups;
   a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0x7FFFFFF0ull) * 2 + 8;
-  // 64: many sources expand a vertex in the same iteration and share its
-  // adjacency read (small windows make each source re-read it)
-  a.delta = o && o->sssp_delta ? o->sssp_delta : 64u;
+  // Wide windows: many sources expand a vertex in the same iteration and
+  // share its adjacency read (small windows make each source re-read it).
+  // RMAT-26, 256 sources, weights 1..64: width 16 -> 36.6 q/s, 64 -> 74.8,
+  // 128 -> 99.3, 256 -> 100.1, unbounded -> 100.1.
+  a.delta = o && o->sssp_delta ? o->sssp_delta : kMsDelta;
   a.growth = o && o->sssp_growth ? o->sssp_growth : kMsGrowth;
 
   thv_stats local{};
@@ -915,11 +947,12 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
     b->h_sources[0] = k;
     memcpy(b->h_sources + 1, sources + first, k * 4);
     THV_CUDA(cudaEventRecord(b->ev0, st));
-    THV_TRY(run_group(g, sssp, a, st, out != nullptr, cfg, launches));
+    THV_TRY(run_group(g, sssp, a, st, want_out, cfg, launches));
     THV_CUDA(cudaEventRecord(b->ev1, st));
-    if (out)
-      THV_CUDA(cudaMemcpyAsync(out + (uint64_t)first * g->nv, b->d_out, (uint64_t)k * g->nv * 4,
-                               cudaMemcpyDeviceToHost, st));
+    for (uint32_t i = 0; want_out && i < k; i++)
+      if (rows[first + i])
+        THV_CUDA(cudaMemcpyAsync(rows[first + i], b->d_out + (uint64_t)i * g->nv, g->nv * 4,
+                                 cudaMemcpyDeviceToHost, st));
     THV_CUDA(cudaStreamSynchronize(st));
     cudaEventElapsedTime(ms_out, b->ev0, b->ev1);
     const MsCtrl &hc = *b->h_ctrl;
@@ -958,7 +991,7 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
     THV_TRY(one_group(first, k, cfg, &ms_, &deep));
     if (deep) {
       // deeper than the u8 level bytes hold: this group one source at a time
-      THV_TRY(fallback_single(g, sources + first, k, st, o, out ? out + (uint64_t)first * g->nv : nullptr,
+      THV_TRY(fallback_single(g, sources + first, k, st, o, rows ? rows + first : nullptr,
                               checksums ? checksums + first : nullptr, local));
       continue;
     }
@@ -970,7 +1003,9 @@ thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
     local.hbm_edge_bytes += hc.hbm_bytes;
     local.link_edge_bytes += hc.link_bytes;
     local.h2d_bytes += (kMsWidth + 1) * 4;
-    local.d2h_bytes += sizeof(MsCtrl) + kMsWidth * 8 + (out ? (uint64_t)k * g->nv * 4 : 0);
+    uint64_t rows_out = 0;
+    for (uint32_t i = 0; want_out && i < k; i++) rows_out += rows[first + i] != nullptr;
+    local.d2h_bytes += sizeof(MsCtrl) + kMsWidth * 8 + rows_out * g->nv * 4;
   }
   local.device_ms += dev_ms;
   local.kernel_launches = launches;

@@ -134,7 +134,8 @@ struct thv_graph {
   thv::Plan plan;
   thv::MinState *ms = nullptr;
   thv::PrState *ps = nullptr;
-  thv::BatchState *bs = nullptr;
+  thv::BatchState *bs = nullptr;              // state of the batched run in progress
+  thv::BatchState *bs_keep[2] = {nullptr, nullptr};  // kept per algorithm: BFS, SSSP
   // last run
   int last_algo = -1;
   size_t device_bytes = 0;
@@ -163,6 +164,9 @@ void pagerank_free(thv_graph *g);
 thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
                      uint32_t n, const thv_batch_opts *o, uint32_t *out,
                      uint64_t *checksums, thv_stats *stats);
+thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
+                          uint32_t n, const thv_batch_opts *o, uint32_t *const *rows,
+                          uint64_t *checksums, thv_stats *stats);
 void batch_free(thv_graph *g);
 
 thv_status generate_rmat(const thv_rmat_opts *o, thv_format fmt, int device,
