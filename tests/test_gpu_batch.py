@@ -129,3 +129,16 @@ def test_autotuner_picks_and_caches_a_configuration(T, O, g14, tmp_path, monkeyp
         out2, sums2, _ = g.batch_run("bfs", src, tune=True)
         assert np.array_equal(sums, sums2)
         assert len(cache.read_text().strip().splitlines()) == 1
+
+
+def test_direct_launches_equal_graph_replays(T, O, g14w, monkeypatch):
+    src = sources(O, g14w, 64)
+    res = {}
+    for direct in ("0", "1"):
+        monkeypatch.setenv("THV_BATCH_DIRECT", direct)
+        with T.Graph.from_arrays(g14w.off, g14w.wcsr_edges(), "wcsr") as g:
+            g.plan(int(0.4 * g.ne * 8), block_bytes=BLOCK)
+            res[direct] = [g.batch_run(a, src, want_values=False, timeout_ms=20000)[1]
+                           for a in ("bfs", "sssp")]
+    for a, b in zip(res["0"], res["1"]):
+        assert np.array_equal(a, b)

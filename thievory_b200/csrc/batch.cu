@@ -609,9 +609,17 @@ struct GraphKey {
   }
 };
 
+// THV_BATCH_DIRECT=1 launches every group directly instead of replaying a
+// captured graph (kernel profilers list cooperative kernels launched from a
+// graph poorly); results are the same either way.
+static bool batch_capture_allowed() {
+  const char *e = getenv("THV_BATCH_DIRECT");
+  return !(e && e[0] == '1');
+}
+
 struct BatchExtra {
   std::map<GraphKey, cudaGraphExec_t> graphs;
-  bool capture_ok = true;
+  bool capture_ok = batch_capture_allowed();
 };
 
 static std::map<BatchState *, BatchExtra> g_extra;  // graphs per batch state
