@@ -185,6 +185,10 @@ typedef struct thv_run_opts {
  * window empties (one barrier per iteration; the default for SSSP). */
 #define THV_RUN_SCAN_COMPACTION 2u
 #define THV_RUN_QUEUE_COMPACTION 4u
+/* BFS on a graph whose out-edges are all resident switches to bottom-up
+ * levels over an in-edge transpose (built in HBM on first use) when the
+ * frontier is large; this flag keeps every level top-down.  Same results. */
+#define THV_RUN_TOP_DOWN_ONLY 8u
 
 typedef struct thv_stats {
   double device_ms;         /* CUDA-event time of the traversal */
@@ -196,7 +200,7 @@ typedef struct thv_stats {
   uint64_t h2d_bytes;       /* explicit host->device copies in the call */
   uint64_t d2h_bytes;       /* explicit device->host copies in the call */
   uint32_t kernel_launches;
-  uint32_t pad;
+  uint32_t bottom_up_levels; /* BFS levels run bottom-up */
   uint64_t checksum;        /* with THV_RUN_CHECKSUM */
 } thv_stats;
 

@@ -55,7 +55,8 @@ def test_bfs(T, O, g14, frac):
             got, st = g.run("bfs", source=src, timeout_ms=20000)
             want = O.bfs(g14, src)
             assert np.array_equal(got, want), f"src {src}"
-            assert st["edges_expanded"] == O.reached_edges(g14, want)
+            if st["bottom_up_levels"] == 0:  # bottom-up levels scan in-edges instead
+                assert st["edges_expanded"] == O.reached_edges(g14, want)
 
 
 @pytest.mark.parametrize("frac", BUDGETS)
@@ -307,3 +308,42 @@ def test_scan_and_queue_compaction_agree(T, O, g14w, frac):
         for mode in ("scan", "queue"):
             got, _ = g.run("cc", compaction=mode, timeout_ms=20000)
             assert np.array_equal(got, O.cc(g14w))
+
+
+def test_bfs_direction_optimising(T, O, g14):
+    """All edges resident: BFS switches to bottom-up levels over the in-edge
+    transpose for large frontiers; values equal the top-down run's."""
+    srcs = O.sources(g14, 4).tolist()
+    with engine_graph(T, g14) as g:
+        plan(g, 1.0)
+        used = 0
+        for s in srcs:
+            want = O.bfs(g14, s)
+            got, st = g.run("bfs", source=s, timeout_ms=20000)
+            assert np.array_equal(got, want), s
+            used += st["bottom_up_levels"]
+            td, st_td = g.run("bfs", source=s, top_down_only=True, timeout_ms=20000)
+            assert np.array_equal(td, want) and st_td["bottom_up_levels"] == 0
+            assert st_td["edges_expanded"] == O.reached_edges(g14, want)
+        assert used > 0
+        plan(g, 0.4)  # host blocks: no transpose, top-down only
+        _, st = g.run("bfs", source=srcs[0], timeout_ms=20000)
+        assert st["bottom_up_levels"] == 0
+
+
+def test_bfs_direction_optimising_symmetric_and_toys(T, O):
+    s = O.rmat(13, 8, symmetric=True)
+    with engine_graph(T, s) as g:
+        plan(g, 1.0)
+        for src in O.sources(s, 3).tolist():
+            got, _ = g.run("bfs", source=src, timeout_ms=20000)
+            assert np.array_equal(got, O.bfs(s, src))
+    # a star whose centre reaches everything in one level, then a path
+    n = 2000
+    src_ = [0] * (n - 1) + list(range(1, n - 1))
+    dst_ = list(range(1, n)) + list(range(2, n))
+    t = O.from_edges(n, src_, dst_)
+    with engine_graph(T, t) as g:
+        plan(g, 1.0)
+        got, _ = g.run("bfs", source=0, timeout_ms=20000)
+        assert np.array_equal(got, O.bfs(t, 0))

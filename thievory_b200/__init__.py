@@ -57,7 +57,7 @@ class _Stats(ctypes.Structure):
                 ("iterations", ctypes.c_uint64), ("edges_expanded", ctypes.c_uint64),
                 ("hbm_edge_bytes", ctypes.c_uint64), ("link_edge_bytes", ctypes.c_uint64),
                 ("h2d_bytes", ctypes.c_uint64), ("d2h_bytes", ctypes.c_uint64),
-                ("kernel_launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+                ("kernel_launches", ctypes.c_uint32), ("bottom_up_levels", ctypes.c_uint32),
                 ("checksum", ctypes.c_uint64)]
 
     def to_dict(self) -> dict:
@@ -282,13 +282,13 @@ class Graph:
             out: Optional[np.ndarray] = None, want_values: bool = True, stream: int = 0,
             sssp_delta: int = 0, timeout_ms: int = 0, small_degree: int = 0,
             chunk_edges: int = 0, checksum: bool = False, compaction: str = "",
-            sssp_growth: int = 0):
+            sssp_growth: int = 0, top_down_only: bool = False):
         """Run algo; returns (values or None, stats dict).  compaction:
         "" (per-algorithm default), "scan" or "queue"; sssp_growth: SSSP
         window growth per advance (0 = default 8, 1 = fixed windows)."""
         lib = load_library()
         flags = ((1 if checksum else 0) | (2 if compaction == "scan" else 0)
-                 | (4 if compaction == "queue" else 0))
+                 | (4 if compaction == "queue" else 0) | (8 if top_down_only else 0))
         o = _RunOpts(source, pr_iters, pr_damping, sssp_delta, timeout_ms,
                      ctypes.c_void_p(stream) if stream else None, small_degree, chunk_edges,
                      flags, sssp_growth)

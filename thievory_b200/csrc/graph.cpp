@@ -119,6 +119,7 @@ static void graph_destroy(thv_graph *g) {
   batch_free(g);
   minprop_free(g);
   pagerank_free(g);
+  transpose_free(g);
   plan_free(g);
   dev_free(g->d_off);
   dev_free(g->d_outdeg);

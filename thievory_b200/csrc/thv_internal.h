@@ -134,6 +134,9 @@ struct thv_graph {
   thv::Plan plan;
   thv::MinState *ms = nullptr;
   thv::PrState *ps = nullptr;
+  uint64_t *d_in_off = nullptr;   // in-edge transpose (direction-optimising BFS)
+  uint32_t *d_in_adj = nullptr;
+  bool in_valid = false;
   thv::BatchState *bs = nullptr;              // state of the batched run in progress
   thv::BatchState *bs_keep[2] = {nullptr, nullptr};  // kept per algorithm: BFS, SSSP
   // last run
@@ -146,6 +149,8 @@ namespace thv {
 
 thv_status graph_init_device(thv_graph *g);  // stream, d_off, d_outdeg
 thv_status set_packing(thv_graph *g, bool on);  // weighted graphs only
+thv_status ensure_transpose(thv_graph *g, cudaStream_t st);  // transpose.cu
+void transpose_free(thv_graph *g);
 thv_status ensure_plan(thv_graph *g);
 thv_status build_tiles(thv_graph *g);
 void plan_free(thv_graph *g);
