@@ -469,6 +469,9 @@ def run_reference(args, dist):
     wl = dict(WORKLOADS[args.workload])
     if args.scale:
         wl["scale"] = args.scale
+    # all host cores: torchrun sets OMP_NUM_THREADS=1 for every rank, and
+    # here rank 0 alone does the work
+    O.set_threads(len(os.sched_getaffinity(0)))
     g = O.rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"], weighted=wl["algo"] == "sssp")
     algo = wl["algo"]
     fn = {"sssp": lambda: O.sssp(g, args.source, parallel=True),

@@ -64,6 +64,7 @@ def lib() -> ctypes.CDLL:
             "thvo_write_values": ([ctypes.c_char_p, P, U64, U32], I),
             "thvo_now": ([], D),
             "thvo_threads": ([], I),
+            "thvo_set_threads": ([I], None),
         }
         for n, (a, r) in sig.items():
             f = getattr(L, n)
@@ -240,3 +241,8 @@ def write_csc(path: str, g: CSR) -> None:
 
 def threads() -> int:
     return int(lib().thvo_threads())
+
+
+def set_threads(n: int) -> None:
+    """OpenMP threads of later oracle calls (a launcher may have set 1)."""
+    lib().thvo_set_threads(int(n))

@@ -612,3 +612,6 @@ double thvo_now(void) {
 }
 
 int thvo_threads(void) { return omp_get_max_threads(); }
+void thvo_set_threads(int n) {
+  if (n > 0) omp_set_num_threads(n);
+}

@@ -131,6 +131,7 @@ int thvo_write_values(const char *path, const void *vals, uint64_t n,
 double thvo_now(void);
 /* Threads OpenMP will use. */
 int thvo_threads(void);
+void thvo_set_threads(int n); /* OpenMP threads for later calls */
 
 #ifdef __cplusplus
 }

@@ -758,30 +758,35 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
   const unsigned incl = warp_incl_scan<unsigned>(cnt);
   const unsigned excl = incl - cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
-  for (unsigned k = 0; k < total; k += 32) {
-    const unsigned t = k + lane;
-    const int o = warp_owner(excl, t);
-    const unsigned long long ea = shfl64(eaddr, o);
-    const unsigned oex = __shfl_sync(kFull, excl, o);
-    const uint32_t ov = __shfl_sync(kFull, vval, o);
-    uint32_t w[1] = {0};
-    unsigned long long cand[1];
-    bool ok[1] = {t < total};
-    uint32_t wt = 0;
-    if (ok[0]) {
-      const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
-      if (ESZ == 4) {
-        const uint32_t ed = ld_nc_u32(addr);
-        w[0] = edge_dst(ed, a.wshift);
-        wt = edge_wt(ed, a.wshift, a.wbase);
-      } else {
-        const uint2 ed = ld_nc_u2(addr);
-        w[0] = ed.x;
-        wt = ed.y;
+  // 64 edges per step, two per lane in flight
+  for (unsigned k = 0; k < total; k += 64) {
+    uint32_t w[2] = {0, 0};
+    unsigned long long cand[2];
+    bool ok[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const unsigned t = k + 32u * h + lane;
+      const int o = warp_owner(excl, t);
+      const unsigned long long ea = shfl64(eaddr, o);
+      const unsigned oex = __shfl_sync(kFull, excl, o);
+      const uint32_t ov = __shfl_sync(kFull, vval, o);
+      ok[h] = t < total;
+      uint32_t wt = 0;
+      if (ok[h]) {
+        const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
+        if (ESZ == 4) {
+          const uint32_t ed = ld_nc_u32(addr);
+          w[h] = edge_dst(ed, a.wshift);
+          wt = edge_wt(ed, a.wshift, a.wbase);
+        } else {
+          const uint2 ed = ld_nc_u2(addr);
+          w[h] = ed.x;
+          wt = ed.y;
+        }
       }
+      cand[h] = candidate<OP>(ov, wt);
     }
-    cand[0] = candidate<OP>(ov, wt);
-    q_relax_n<OP, ESZ, 1>(a, e, w, cand, ok, qst);
+    q_relax_n<OP, ESZ, 2>(a, e, w, cand, ok, qst);
   }
 }
 
