@@ -103,6 +103,19 @@ thv_status thv_generate_rmat(const thv_rmat_opts *o, thv_format fmt,
                              int device, thv_graph **out);
 
 thv_status thv_save(const thv_graph *g, const char *path);
+
+/* Text edge list -> .csr / .csc / .wcsr, sorting on the GPU; the bytes of
+ * converter/converter.cpp (ConvertTxtToBCSR :676-808, ConvertTxtToBCSC
+ * :483-589).  The first skip_lines lines are dropped; each later line is
+ * "src dst [w]" (w read with THV_CONVERT_WEIGHTED, else 20); a field that
+ * does not parse keeps the previous line's value, as the converter's
+ * stream does.  Duplicates and self-loops are kept; nv = max id + 1.
+ * nv_out / ne_out may be NULL. */
+#define THV_CONVERT_WEIGHTED 1u   /* third column is the weight (-DWEIGHTED) */
+#define THV_CONVERT_UNDIRECTED 2u /* add dst -> src for every line (-DUNDIRECTED) */
+thv_status thv_convert(const char *txt_path, const char *out_path, thv_format fmt,
+                       uint32_t skip_lines, uint32_t flags, int device,
+                       uint64_t *nv_out, uint64_t *ne_out);
 thv_status thv_close(thv_graph *g);
 
 typedef struct thv_graph_info {

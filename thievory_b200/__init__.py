@@ -116,7 +116,7 @@ class _QueryStats(ctypes.Structure):
 # Every function include/thv.h declares (tests check the library exports them).
 ABI_FUNCTIONS = [
     "thv_open", "thv_from_arrays", "thv_generate_rmat", "thv_save", "thv_close",
-    "thv_info", "thv_set_edge_packing", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_run",
+    "thv_info", "thv_set_edge_packing", "thv_convert", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_run",
     "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
     "thv_pick_sources", "thv_bfs_noalloc", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
@@ -145,6 +145,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_close": ([P], I32),
         "thv_info": ([P, ctypes.POINTER(_GraphInfo)], I32),
         "thv_set_edge_packing": ([P, I32], I32),
+        "thv_convert": ([ctypes.c_char_p, ctypes.c_char_p, U32, U32, U32, I32,
+                         ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)], I32),
         "thv_host_arrays": ([P, pp, pp, pp], I32),
         "thv_plan": ([P, ctypes.POINTER(_PlanOpts)], I32),
         "thv_get_plan": ([P, ctypes.POINTER(_PlanInfo)], I32),
@@ -187,6 +189,17 @@ def _ptr(a: np.ndarray) -> ctypes.c_void_p:
 
 def value_dtype(algo: str):
     return np.float64 if algo.startswith("pr") else np.uint32
+
+
+def convert(txt_path: str, out_path: str, fmt: str = "csr", skip: int = 4,
+            weighted: bool = False, undirected: bool = False, device: int = 0):
+    """Text edge list -> .csr/.csc/.wcsr with the reference converter's bytes
+    (converter/converter.cpp); sorts on the GPU.  Returns (nv, ne)."""
+    nv, ne = ctypes.c_uint64(), ctypes.c_uint64()
+    flags = (1 if weighted else 0) | (2 if undirected else 0)
+    _check(load_library().thv_convert(txt_path.encode(), out_path.encode(), FMT[fmt], skip, flags,
+                                      device, ctypes.byref(nv), ctypes.byref(ne)), "thv_convert")
+    return int(nv.value), int(ne.value)
 
 
 class Graph:

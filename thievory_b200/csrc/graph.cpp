@@ -758,6 +758,14 @@ thv_status thv_info(const thv_graph *g, thv_graph_info *o) {
   return THV_OK;
 }
 
+thv_status thv_convert(const char *txt_path, const char *out_path, thv_format fmt,
+                       uint32_t skip_lines, uint32_t flags, int device, uint64_t *nv_out,
+                       uint64_t *ne_out) {
+  THV_GUARD_BEGIN
+  return convert_edge_list(txt_path, out_path, fmt, skip_lines, flags, device, nv_out, ne_out);
+  THV_GUARD_END
+}
+
 thv_status thv_set_edge_packing(thv_graph *g, int packed) {
   THV_GUARD_BEGIN
   if (!g) return fail(THV_EINVAL, "null graph");

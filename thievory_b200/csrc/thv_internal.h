@@ -150,6 +150,9 @@ namespace thv {
 thv_status graph_init_device(thv_graph *g);  // stream, d_off, d_outdeg
 thv_status set_packing(thv_graph *g, bool on);  // weighted graphs only
 thv_status ensure_transpose(thv_graph *g, cudaStream_t st);  // transpose.cu
+thv_status convert_edge_list(const char *txt, const char *out_path, thv_format fmt,
+                             uint32_t skip, uint32_t flags, int device, uint64_t *nv_out,
+                             uint64_t *ne_out);  // convert.cu
 void transpose_free(thv_graph *g);
 thv_status ensure_plan(thv_graph *g);
 thv_status build_tiles(thv_graph *g);
