@@ -141,6 +141,9 @@ thv_status thv_host_arrays(const thv_graph *g, const uint64_t **off,
 /* ---- placement plan (static HBM budget) ---- */
 #define THV_PLACE_DENSEST 0u /* resident blocks chosen by edges per vertex */
 #define THV_PLACE_PREFIX 1u  /* longest prefix of blocks (reference order) */
+#define THV_PLACE_ACCESS 2u  /* blocks whose adjacency was read the most per
+                                byte under earlier tracked plans first (then
+                                densest) */
 
 typedef struct thv_plan_opts {
   uint64_t hbm_budget_bytes; /* resident edge bytes; UINT64_MAX = all that fit */
@@ -154,7 +157,16 @@ typedef struct thv_plan_opts {
    * read the cache; PageRank reads whole blocks and ignores it.
    * 0 = default (64 for CSR/WCSR, off for CSC); 1 = off. */
   uint32_t small_list_degree;
+  uint32_t flags; /* THV_PLAN_* */
+  uint32_t pad;
 } thv_plan_opts;
+
+/* thv_plan_opts.flags: count, per block, the adjacency bytes the traversal
+ * kernels read from it, resident or over the link (thv_get_block_access);
+ * the counts carry over to later plans of the graph for THV_PLACE_ACCESS.  Replaces
+ * the reference's lazy caching of filtered partitions (src/bfs/bfs.cu:
+ * 155-519) with measured, explicit re-placement. */
+#define THV_PLAN_TRACK_ACCESS 1u
 
 typedef struct thv_plan_info {
   uint64_t num_blocks, resident_blocks;
@@ -171,6 +183,16 @@ thv_status thv_get_plan(const thv_graph *g, thv_plan_info *out);
  * the capacity of resident (vbegin needs cap + 1); *nb receives the count. */
 thv_status thv_get_blocks(const thv_graph *g, uint64_t cap, uint32_t *vbegin,
                           uint8_t *resident, uint64_t *nb);
+/* Adjacency bytes read from each block since this plan was made, from HBM
+ * or over the link (tracked plans).  bytes has cap entries. */
+thv_status thv_get_block_access(const thv_graph *g, uint64_t cap, uint64_t *bytes,
+                                uint64_t *nb);
+/* Plan persistence: the block split, the resident set, the small-list
+ * threshold and the access counts.  Loading re-creates exactly that plan
+ * on the same graph (same vertex, edge and stored-edge sizes; otherwise
+ * THV_EINVAL) and keeps the counts for THV_PLACE_ACCESS. */
+thv_status thv_save_plan(const thv_graph *g, const char *path);
+thv_status thv_load_plan(thv_graph *g, const char *path);
 
 /* ---- single-source / whole-graph runs ---- */
 typedef struct thv_run_opts {
@@ -272,7 +294,9 @@ typedef struct thv_serve_opts {
                                 as batched groups of up to 64 (the
                                 thv_batch_run kernels) instead of slots;
                                 0 = 2, 0xFFFFFFFF = never (slots only) */
-  uint32_t pad;
+  uint32_t replan_every;     /* re-place the graph's blocks by measured
+                                access (THV_PLACE_ACCESS, same budget) after
+                                this many finished queries; 0 = never */
 } thv_serve_opts;
 
 typedef struct thv_query_stats {

@@ -34,7 +34,7 @@ THV_ETIMEOUT, THV_EUNSUPPORTED, THV_EBUSY, THV_ENOTREADY, THV_EDEVICE = 6, 7, 8,
 
 FMT = {"csr": 0, "csc": 1, "wcsr": 2}
 ALGO = {"bfs": 0, "cc": 1, "sssp": 2, "pr_push": 3, "pr_pull": 4}
-PLACE = {"densest": 0, "prefix": 1}
+PLACE = {"densest": 0, "prefix": 1, "access": 2}
 OPEN_WEIGHTS = 1
 
 
@@ -66,7 +66,8 @@ class _Stats(ctypes.Structure):
 
 class _PlanOpts(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("block_bytes", ctypes.c_uint64),
-                ("policy", ctypes.c_uint32), ("small_list_degree", ctypes.c_uint32)]
+                ("policy", ctypes.c_uint32), ("small_list_degree", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
 
 
 class _PlanInfo(ctypes.Structure):
@@ -100,7 +101,7 @@ class _ServeOpts(ctypes.Structure):
     _fields_ = [("max_slots", ctypes.c_uint32), ("queue_capacity", ctypes.c_uint32),
                 ("mem_budget_bytes", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32),
                 ("max_batch_iters", ctypes.c_uint32), ("group_min", ctypes.c_uint32),
-                ("pad", ctypes.c_uint32)]
+                ("replan_every", ctypes.c_uint32)]
 
 
 class _QueryStats(ctypes.Structure):
@@ -116,7 +117,7 @@ class _QueryStats(ctypes.Structure):
 # Every function include/thv.h declares (tests check the library exports them).
 ABI_FUNCTIONS = [
     "thv_open", "thv_from_arrays", "thv_generate_rmat", "thv_save", "thv_close",
-    "thv_info", "thv_set_edge_packing", "thv_convert", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_run",
+    "thv_info", "thv_set_edge_packing", "thv_convert", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_get_block_access", "thv_save_plan", "thv_load_plan", "thv_run",
     "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
     "thv_pick_sources", "thv_bfs_noalloc", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
@@ -151,6 +152,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_plan": ([P, ctypes.POINTER(_PlanOpts)], I32),
         "thv_get_plan": ([P, ctypes.POINTER(_PlanInfo)], I32),
         "thv_get_blocks": ([P, U64, P, P, ctypes.POINTER(ctypes.c_uint64)], I32),
+        "thv_get_block_access": ([P, U64, P, ctypes.POINTER(ctypes.c_uint64)], I32),
+        "thv_save_plan": ([P, ctypes.c_char_p], I32),
+        "thv_load_plan": ([P, ctypes.c_char_p], I32),
         "thv_link_bandwidth": ([I32, U64, ctypes.POINTER(D), ctypes.POINTER(D)], I32),
         "thv_pick_sources": ([P, U64, U32, P], I32),
         "thv_bfs_noalloc": ([P, P, U64, U64, U32, P, P, ctypes.POINTER(ctypes.c_uint64)], I32),
@@ -264,13 +268,17 @@ class Graph:
 
     # -- plan ---------------------------------------------------------------
     def plan(self, hbm_budget_bytes: Optional[int] = None, block_bytes: int = 0,
-             policy: str = "densest", small_list_degree: int = 0) -> dict:
+             policy: str = "densest", small_list_degree: int = 0,
+             track_access: bool = False) -> dict:
         """Choose the HBM-resident edges.  small_list_degree: lists shorter
         than this in host blocks are cached in HBM first (0 = default: 64
-        for CSR/WCSR, off for CSC; 1 = off; PageRank ignores the cache)."""
+        for CSR/WCSR, off for CSC; 1 = off; PageRank ignores the cache).
+        policy "access" keeps the blocks that read the most link bytes
+        under earlier plans made with track_access."""
         lib = load_library()
         o = _PlanOpts(2**64 - 1 if hbm_budget_bytes is None else int(hbm_budget_bytes),
-                      int(block_bytes), PLACE[policy], int(small_list_degree))
+                      int(block_bytes), PLACE[policy], int(small_list_degree),
+                      1 if track_access else 0, 0)
         _check(lib.thv_plan(self._h, ctypes.byref(o)), "thv_plan")
         return self.plan_info()
 
@@ -278,6 +286,24 @@ class Graph:
         pi = _PlanInfo()
         _check(load_library().thv_get_plan(self._h, ctypes.byref(pi)), "thv_get_plan")
         return {k: int(getattr(pi, k)) for k, _ in pi._fields_}
+
+    def block_access(self) -> np.ndarray:
+        """Adjacency bytes read from each block (HBM or link) under the
+        current tracked plan."""
+        lib = load_library()
+        nb = ctypes.c_uint64()
+        _check(lib.thv_get_block_access(self._h, 0, None, ctypes.byref(nb)), "thv_get_block_access")
+        out = np.zeros(nb.value, np.uint64)
+        _check(lib.thv_get_block_access(self._h, nb.value, _ptr(out), ctypes.byref(nb)),
+               "thv_get_block_access")
+        return out
+
+    def save_plan(self, path: str) -> None:
+        _check(load_library().thv_save_plan(self._h, path.encode()), "thv_save_plan")
+
+    def load_plan(self, path: str) -> dict:
+        _check(load_library().thv_load_plan(self._h, path.encode()), "thv_load_plan")
+        return self.plan_info()
 
     def blocks(self):
         """(vbegin[nb+1] u32, resident[nb] bool) of the current plan."""
@@ -386,14 +412,14 @@ class Server:
 
     def __init__(self, graph: Graph, max_slots: int = 64, queue_capacity: int = 0,
                  mem_budget_bytes: int = 0, timeout_ms: int = 0, max_batch_iters: int = 0,
-                 group_min: int = 0):
+                 group_min: int = 0, replan_every: int = 0):
         """group_min: queue depth from which waiting queries run as batched
         groups (0 = 2, 0xFFFFFFFF = never: slots only)."""
         lib = load_library()
         self.graph = graph
         self._bufs = {}
         o = _ServeOpts(max_slots, queue_capacity, mem_budget_bytes, timeout_ms, max_batch_iters,
-                       group_min, 0)
+                       group_min, replan_every)
         self._h = ctypes.c_void_p()
         _check(lib.thv_serve_start(graph._h, ctypes.byref(o), ctypes.byref(self._h)),
                "thv_serve_start")

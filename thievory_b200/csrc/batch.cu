@@ -53,6 +53,7 @@ struct MsArgs {
   const uint64_t *blk_base;
   uint64_t host_base;
   ListCache lc;
+  unsigned long long *blk_access;  // tracked plans: adjacency bytes read per block
   unsigned long long *visit;  // BFS
   unsigned long long *front;  // pending (vertex, source) pairs
   uint8_t *lvl;               // BFS [nv][64]: level + 1, 0 = unreached
@@ -386,8 +387,9 @@ __global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
           const uint64_t s0 = __ldg(a.off + v), e0 = __ldg(a.off + v + 1);
           deg = (uint32_t)(e0 - s0);
           bool host;
-          eaddr = list_addr(a.lc, __ldg(a.blk_base + find_block(vb, a.nblk, v)), a.host_base, v,
-                            s0, deg, ESZ, &host);
+          const uint32_t bi = find_block(vb, a.nblk, v);
+          eaddr = list_addr(a.lc, __ldg(a.blk_base + bi), a.host_base, v, s0, deg, ESZ, &host);
+          if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
           my_edges += deg;
           my_pairs += __popcll(take);
           if (host) my_link += (unsigned long long)deg * ESZ;
@@ -913,6 +915,7 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
   a.blk_base = g->plan.d_base;
   a.host_base = g->h_edges_dev;
   a.lc = list_cache_of(g->plan);
+  a.blk_access = g->plan.d_access;
   a.wshift = g->wshift;
   a.wbase = g->wbase;
   a.visit = b->d_visit;

@@ -313,8 +313,47 @@ static thv_status open_file(const char *path, thv_format fmt, uint32_t flags,
 
 // ------------------------------------------------------------------ plan --
 
+// Access bytes of old blocks [ovb[i], ovb[i+1]) spread over new blocks by
+// vertex overlap.
+static std::vector<uint64_t> spread_access(const std::vector<uint32_t> &ovb,
+                                           const std::vector<uint64_t> &ob,
+                                           const std::vector<uint32_t> &nvb) {
+  std::vector<uint64_t> out(nvb.empty() ? 0 : nvb.size() - 1, 0);
+  size_t j = 0;
+  for (size_t i = 0; i < ob.size(); i++) {
+    const uint64_t a = ovb[i], b = ovb[i + 1];
+    if (b <= a || !ob[i]) continue;
+    while (j + 1 < nvb.size() && nvb[j + 1] <= a) j++;
+    for (size_t k = j; k + 1 < nvb.size() && nvb[k] < b; k++) {
+      const uint64_t lo = std::max<uint64_t>(a, nvb[k]), hi = std::min<uint64_t>(b, nvb[k + 1]);
+      if (hi > lo) out[k] += (uint64_t)((__uint128_t)ob[i] * (hi - lo) / (b - a));
+    }
+  }
+  return out;
+}
+
+// Folds the counters of a tracked plan into the graph's access history.
+static void fold_access(thv_graph *g) {
+  Plan &p = g->plan;
+  if (!p.d_access || p.blocks.empty()) return;
+  std::vector<uint64_t> cur(p.blocks.size(), 0);
+  if (cudaMemcpy(cur.data(), p.d_access, cur.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  std::vector<uint32_t> vb(p.vbegin.begin(), p.vbegin.end());
+  if (!g->access_bytes.empty()) {
+    const std::vector<uint64_t> old = spread_access(g->access_vb, g->access_bytes, vb);
+    for (size_t i = 0; i < cur.size(); i++) cur[i] += old[i];
+  }
+  g->access_vb = vb;
+  g->access_bytes = cur;
+}
+
 void plan_free(thv_graph *g) {
   Plan &p = g->plan;
+  fold_access(g);
+  dev_free(p.d_access);
   dev_free(p.d_resident);
   dev_free(p.d_lists);
   dev_free(p.d_list_idx);
@@ -393,7 +432,9 @@ static thv_status build_list_cache(thv_graph *g, uint32_t ldeg) {
   return st;
 }
 
-static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
+// force: an explicit resident flag per block (a loaded plan), or null.
+static thv_status do_plan(thv_graph *g, const thv_plan_opts *o,
+                          const std::vector<uint8_t> *force = nullptr) {
   THV_CUDA(cudaSetDevice(g->device));
   if (g->stream) THV_CUDA(cudaStreamSynchronize(g->stream));
   batch_free(g);  // its captured launch graphs hold the old plan's tables
@@ -402,6 +443,8 @@ static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
   const uint64_t esz = g->esz;
   p.block_bytes = o && o->block_bytes ? o->block_bytes : kDefaultBlockBytes;
   p.policy = o ? o->policy : THV_PLACE_DENSEST;
+  p.flags = o ? o->flags : 0;
+  if (p.policy > THV_PLACE_ACCESS) return fail(THV_EINVAL, "unknown placement policy %u", p.policy);
   const uint64_t max_edges = std::max<uint64_t>(1, p.block_bytes / esz);
   // blocks on vertex boundaries (src/graph.cuh:270-304)
   uint32_t begin = 0;
@@ -462,26 +505,53 @@ static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
   }
   std::vector<uint32_t> order(p.blocks.size());
   std::iota(order.begin(), order.end(), 0u);
+  auto denser = [&](uint32_t x, uint32_t y) {
+    const Block &a = p.blocks[x], &b = p.blocks[y];
+    // edges per vertex, compared without division
+    const __uint128_t l = (__uint128_t)(a.eend - a.ebegin) * std::max<uint64_t>(1, b.vend - b.vbegin);
+    const __uint128_t r = (__uint128_t)(b.eend - b.ebegin) * std::max<uint64_t>(1, a.vend - a.vbegin);
+    return l > r;
+  };
   if (p.policy == THV_PLACE_DENSEST) {
+    std::stable_sort(order.begin(), order.end(), denser);
+  } else if (p.policy == THV_PLACE_ACCESS) {
+    // most adjacency bytes read per byte of HBM the block would take (its
+    // long lists)
+    std::vector<uint32_t> vb(p.blocks.size() + 1);
+    for (size_t b = 0; b < p.blocks.size(); b++) vb[b] = p.blocks[b].vbegin;
+    vb[p.blocks.size()] = (uint32_t)g->nv;
+    const std::vector<uint64_t> hot =
+        g->access_bytes.empty() ? std::vector<uint64_t>(p.blocks.size(), 0)
+                                : spread_access(g->access_vb, g->access_bytes, vb);
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-      const Block &a = p.blocks[x], &b = p.blocks[y];
-      // edges per vertex, compared without division
-      const __uint128_t l = (__uint128_t)(a.eend - a.ebegin) * std::max<uint64_t>(1, b.vend - b.vbegin);
-      const __uint128_t r = (__uint128_t)(b.eend - b.ebegin) * std::max<uint64_t>(1, a.vend - a.vbegin);
-      return l > r;
+      const uint64_t cx = std::max<uint64_t>(1, (p.blocks[x].eend - p.blocks[x].ebegin) * esz - small_b[x]);
+      const uint64_t cy = std::max<uint64_t>(1, (p.blocks[y].eend - p.blocks[y].ebegin) * esz - small_b[y]);
+      const __uint128_t l = (__uint128_t)hot[x] * cy, r = (__uint128_t)hot[y] * cx;
+      if (l != r) return l > r;
+      return denser(x, y);
     });
   }
   // the cache is paid first; a block then costs only its long lists
   uint64_t used = small_total;
-  for (uint32_t b : order) {
-    const uint64_t bytes = (p.blocks[b].eend - p.blocks[b].ebegin) * esz;
-    if (bytes == 0) continue;
-    const uint64_t cost = bytes - small_b[b];
-    if (used + cost <= budget) {
+  if (force) {
+    if (force->size() != p.blocks.size()) return fail(THV_EINVAL, "plan has a different block split");
+    for (size_t b = 0; b < p.blocks.size(); b++) {
+      if (!(*force)[b]) continue;
       p.blocks[b].resident = true;
-      used += cost;
-    } else if (p.policy == THV_PLACE_PREFIX) {
-      break;
+      used += (p.blocks[b].eend - p.blocks[b].ebegin) * esz - small_b[b];
+    }
+    if (used > budget) return fail(THV_EINVAL, "loaded plan exceeds its budget");
+  } else {
+    for (uint32_t b : order) {
+      const uint64_t bytes = (p.blocks[b].eend - p.blocks[b].ebegin) * esz;
+      if (bytes == 0) continue;
+      const uint64_t cost = bytes - small_b[b];
+      if (used + cost <= budget) {
+        p.blocks[b].resident = true;
+        used += cost;
+      } else if (p.policy == THV_PLACE_PREFIX) {
+        break;
+      }
     }
   }
   // pack resident blocks; element offsets keep the edge index's position
@@ -521,7 +591,85 @@ static thv_status do_plan(thv_graph *g, const thv_plan_opts *o) {
   THV_TRY(dev_alloc((void **)&p.d_base, nb * 8, "block table"));
   THV_CUDA(cudaMemcpy(p.d_vbegin, p.vbegin.data(), (nb + 1) * 4, cudaMemcpyHostToDevice));
   THV_CUDA(cudaMemcpy(p.d_base, p.base.data(), nb * 8, cudaMemcpyHostToDevice));
+  if (p.flags & THV_PLAN_TRACK_ACCESS) {
+    THV_TRY(dev_alloc((void **)&p.d_access, nb * 8, "block access counters"));
+    THV_CUDA(cudaMemset(p.d_access, 0, nb * 8));
+  }
   p.valid = true;
+  return THV_OK;
+}
+
+// Re-places blocks by the measured access with the current plan's budget,
+// block size, small-list threshold and flags.
+thv_status replan_by_access(thv_graph *g) {
+  if (!g->plan.valid) return THV_OK;
+  thv_plan_opts o{};
+  o.hbm_budget_bytes = g->plan.budget_bytes;
+  o.block_bytes = g->plan.block_bytes;
+  o.policy = THV_PLACE_ACCESS;
+  o.small_list_degree = g->plan.list_deg ? g->plan.list_deg : 1u;
+  o.flags = g->plan.flags;
+  return do_plan(g, &o);
+}
+
+// ---- plan files: magic, sizes, options, block split, resident set, access
+static constexpr char kPlanMagic[8] = {'T', 'H', 'V', 'P', 'L', 'A', 'N', '1'};
+
+static thv_status save_plan(const thv_graph *g, const char *path) {
+  const Plan &p = g->plan;
+  if (!p.valid) return fail(THV_EINVAL, "graph has no plan yet");
+  std::vector<uint64_t> acc(p.blocks.size(), 0);
+  if (p.d_access)
+    THV_CUDA(cudaMemcpy(acc.data(), p.d_access, acc.size() * 8, cudaMemcpyDeviceToHost));
+  if (!g->access_bytes.empty()) {
+    std::vector<uint32_t> vb(p.vbegin.begin(), p.vbegin.end());
+    const std::vector<uint64_t> old = spread_access(g->access_vb, g->access_bytes, vb);
+    for (size_t i = 0; i < acc.size(); i++) acc[i] += old[i];
+  }
+  std::unique_ptr<FILE, FileCloser> f(fopen(path, "wb"));
+  if (!f) return fail(THV_EIO, "cannot create %s: %s", path, strerror(errno));
+  const uint64_t hdr[8] = {g->nv, g->ne, g->esz, p.block_bytes, p.budget_bytes,
+                           p.list_deg ? p.list_deg : 1u, p.flags, p.blocks.size()};
+  std::vector<uint8_t> res(p.blocks.size());
+  for (size_t i = 0; i < res.size(); i++) res[i] = p.blocks[i].resident ? 1 : 0;
+  bool ok = fwrite(kPlanMagic, 1, 8, f.get()) == 8 && fwrite(hdr, 8, 8, f.get()) == 8 &&
+            fwrite(p.vbegin.data(), 4, p.vbegin.size(), f.get()) == p.vbegin.size() &&
+            fwrite(res.data(), 1, res.size(), f.get()) == res.size() &&
+            fwrite(acc.data(), 8, acc.size(), f.get()) == acc.size();
+  if (!ok) return fail(THV_EIO, "write to %s failed", path);
+  return THV_OK;
+}
+
+static thv_status load_plan(thv_graph *g, const char *path) {
+  std::unique_ptr<FILE, FileCloser> f(fopen(path, "rb"));
+  if (!f) return fail(THV_EIO, "cannot open %s: %s", path, strerror(errno));
+  char magic[8];
+  uint64_t hdr[8];
+  if (fread(magic, 1, 8, f.get()) != 8 || memcmp(magic, kPlanMagic, 8) != 0 ||
+      fread(hdr, 8, 8, f.get()) != 8)
+    return fail(THV_EFORMAT, "%s: not a plan file", path);
+  if (hdr[0] != g->nv || hdr[1] != g->ne || hdr[2] != g->esz)
+    return fail(THV_EINVAL, "%s: plan of another graph (n=%llu m=%llu edge size %llu)", path,
+                (unsigned long long)hdr[0], (unsigned long long)hdr[1],
+                (unsigned long long)hdr[2]);
+  const uint64_t nb = hdr[7];
+  if (nb == 0 || nb > g->nv + 1) return fail(THV_EFORMAT, "%s: bad block count", path);
+  std::vector<uint32_t> vb(nb + 1);
+  std::vector<uint8_t> res(nb);
+  std::vector<uint64_t> acc(nb);
+  if (fread(vb.data(), 4, nb + 1, f.get()) != nb + 1 || fread(res.data(), 1, nb, f.get()) != nb ||
+      fread(acc.data(), 8, nb, f.get()) != nb)
+    return fail(THV_EFORMAT, "%s: truncated plan", path);
+  thv_plan_opts o{};
+  o.block_bytes = hdr[3];
+  o.hbm_budget_bytes = hdr[4];
+  o.small_list_degree = (uint32_t)hdr[5];
+  o.flags = (uint32_t)hdr[6];
+  o.policy = THV_PLACE_DENSEST;
+  THV_TRY(do_plan(g, &o, &res));
+  if (g->plan.vbegin != vb) return fail(THV_EINVAL, "%s: block split differs from this graph's", path);
+  g->access_vb = vb;
+  g->access_bytes = acc;
   return THV_OK;
 }
 
@@ -810,6 +958,34 @@ thv_status thv_get_plan(const thv_graph *g, thv_plan_info *o) {
   o->small_list_bytes = p.list_bytes;
   o->small_list_vertices = p.list_vertices;
   return THV_OK;
+}
+
+thv_status thv_get_block_access(const thv_graph *g, uint64_t cap, uint64_t *link_bytes,
+                                uint64_t *nb) {  // link_bytes: all adjacency bytes read
+  if (!g || !nb) return fail(THV_EINVAL, "null argument");
+  if (!g->plan.valid) return fail(THV_EINVAL, "graph has no plan yet");
+  const Plan &p = g->plan;
+  *nb = p.blocks.size();
+  if (!link_bytes) return THV_OK;
+  if (!p.d_access) return fail(THV_EINVAL, "plan does not track access (THV_PLAN_TRACK_ACCESS)");
+  if (cap < p.blocks.size()) return fail(THV_EINVAL, "capacity %llu < %zu blocks",
+                                         (unsigned long long)cap, p.blocks.size());
+  THV_CUDA(cudaMemcpy(link_bytes, p.d_access, p.blocks.size() * 8, cudaMemcpyDeviceToHost));
+  return THV_OK;
+}
+
+thv_status thv_save_plan(const thv_graph *g, const char *path) {
+  THV_GUARD_BEGIN
+  if (!g || !path) return fail(THV_EINVAL, "null argument");
+  return save_plan(g, path);
+  THV_GUARD_END
+}
+
+thv_status thv_load_plan(thv_graph *g, const char *path) {
+  THV_GUARD_BEGIN
+  if (!g || !path) return fail(THV_EINVAL, "null argument");
+  return load_plan(g, path);
+  THV_GUARD_END
 }
 
 thv_status thv_get_blocks(const thv_graph *g, uint64_t cap, uint32_t *vbegin,

@@ -100,6 +100,7 @@ struct MinArgs {
   const uint64_t *blk_base;
   uint64_t host_base, host_end;  // zero-copy edge range [host_base, host_end)
   ListCache lc;
+  unsigned long long *blk_access;  // tracked plans: adjacency bytes read per block
   MinItem *qs, *qb;
   unsigned long long cap_s, cap_b;
   MinCtrl *ctrl;
@@ -398,8 +399,9 @@ __global__ void __launch_bounds__(kMinThreads)
           const uint64_t s = __ldg(a.off + v), e = __ldg(a.off + v + 1);
           deg = (uint32_t)(e - s);
           bool host;
-          eaddr = list_addr(a.lc, bbase[find_block(vb, a.nblk, v)], a.host_base, v, s, deg, ESZ,
-                            &host);
+          const uint32_t bi = find_block(vb, a.nblk, v);
+          eaddr = list_addr(a.lc, bbase[bi], a.host_base, v, s, deg, ESZ, &host);
+          if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
           my_edges += deg;
           my_verts += 1;
           if (host) my_link += (unsigned long long)deg * ESZ;
@@ -604,8 +606,9 @@ __device__ __forceinline__ void q_append(const MinArgs &a, const uint32_t *vb,
     const uint64_t s0 = __ldg(a.off + w), e0 = __ldg(a.off + w + 1);
     deg = (uint32_t)(e0 - s0);
     bool host;
-    eaddr = list_addr(a.lc, bbase[find_block(vb, a.nblk, w)], a.host_base, w, s0, deg, ESZ,
-                      &host);
+    const uint32_t bi = find_block(vb, a.nblk, w);
+    eaddr = list_addr(a.lc, bbase[bi], a.host_base, w, s0, deg, ESZ, &host);
+    if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
   }
   const bool small = flag && deg > 0 && deg < a.small_deg;
   const bool big = flag && deg >= a.small_deg;
@@ -1074,6 +1077,7 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.host_base = g->h_edges_dev;
   a.host_end = g->h_edges_dev + g->h_edges_bytes;
   a.lc = list_cache_of(g->plan);
+  a.blk_access = g->plan.d_access;
   a.qs = ms->d_qs;
   a.qb = ms->d_qb;
   a.qs2 = ms->d_qs2;

@@ -55,6 +55,7 @@ struct SvArgs {
   const uint64_t *blk_base;
   uint64_t host_base;
   ListCache lc;
+  unsigned long long *blk_access;  // tracked plans: adjacency bytes read per block
   uint32_t *val;  // [nv][W]
   unsigned long long *front;
   uint32_t *bm;
@@ -292,8 +293,9 @@ __global__ void __launch_bounds__(kSvThreads) sv_kernel(SvArgs a) {
           const uint64_t s0 = __ldg(a.off + v), e0 = __ldg(a.off + v + 1);
           deg = (uint32_t)(e0 - s0);
           bool host;
-          eaddr = list_addr(a.lc, __ldg(a.blk_base + find_block(vb, a.nblk, v)), a.host_base, v,
-                            s0, deg, ESZ, &host);
+          const uint32_t bi = find_block(vb, a.nblk, v);
+          eaddr = list_addr(a.lc, __ldg(a.blk_base + bi), a.host_base, v, s0, deg, ESZ, &host);
+          if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
           my_edges += deg;
           my_pairs += __popcll(take);
           if (host) my_link += (unsigned long long)deg * ESZ;
@@ -491,6 +493,8 @@ struct thv_server {
   thv_graph *g = nullptr;
   uint32_t W = 0, queue_cap = 0, batch_iters = 4;
   uint32_t group_min = 0;  // 0: group mode off
+  uint32_t replan_every = 0;        // queries between access re-placements
+  uint64_t done_since_replan = 0;
   uint64_t timeout_ns = 0;
   // device state
   uint32_t *d_val = nullptr, *d_bm = nullptr, *d_out = nullptr;
@@ -550,6 +554,7 @@ SvArgs make_args(thv_server *s) {
   a.blk_base = g->plan.d_base;
   a.host_base = g->h_edges_dev;
   a.lc = list_cache_of(g->plan);
+  a.blk_access = g->plan.d_access;
   // 4-byte edges: packed weights, or unit weights for an unweighted graph
   a.wshift = g->wshift;
   a.wbase = g->packed ? g->wbase : 1u;
@@ -632,6 +637,7 @@ thv_status retire(thv_server *s, unsigned long long done) {
     s->active &= ~(1ull << slot);
     s->unit &= ~(1ull << slot);
     s->slot_ticket[slot] = 0;
+    s->done_since_replan++;
   }
   s->cv_done.notify_all();
   return THV_OK;
@@ -685,6 +691,7 @@ thv_status run_grouped(thv_server *s, thv_algo algo, const std::vector<uint64_t>
     q.done = true;
   }
   s->total_iters += bst.iterations;
+  s->done_since_replan += n;
   s->cv_done.notify_all();
   return st;
 }
@@ -715,6 +722,7 @@ thv_status run_alone(thv_server *s, thv_algo algo, uint64_t ticket) {
   q.status = st;
   q.done = true;
   s->total_iters += st1.iterations;
+  s->done_since_replan++;
   s->cv_done.notify_all();
   return st;
 }
@@ -726,10 +734,29 @@ void worker_loop(thv_server *s) {
     bool requests_waiting = false;
     std::vector<uint64_t> group;
     thv_algo galgo = THV_ALGO_BFS;
+    bool replan = false;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       s->cv_work.wait(lk, [&] { return s->stopping || !s->waiting.empty() || s->active; });
       if (s->stopping && s->waiting.empty() && !s->active) return;
+      // between queries (no slot running), re-place the edge blocks by the
+      // access this server measured
+      if (s->replan_every && !s->active && s->done_since_replan >= s->replan_every &&
+          (s->g->plan.flags & THV_PLAN_TRACK_ACCESS)) {
+        s->done_since_replan = 0;
+        replan = true;
+      }
+    }
+    if (replan) {
+      const thv_status st = replan_by_access(s->g);
+      if (st != THV_OK) {
+        fail_all(s, st, thv_last_error());
+        return;
+      }
+      continue;
+    }
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
       // A deep queue runs as batched groups: stop admitting into slots, and
       // once the slots have drained take up to 64 waiting queries of the
       // front query's algorithm (FIFO within that algorithm).
@@ -839,6 +866,7 @@ thv_status start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
   s->batch_iters = o && o->max_batch_iters ? o->max_batch_iters : 4u;
   s->group_min = o && o->group_min ? (o->group_min == 0xFFFFFFFFu ? 0u : o->group_min)
                                    : kDefaultGroupMin;
+  s->replan_every = o ? o->replan_every : 0;
   if (o && o->mem_budget_bytes && o->mem_budget_bytes < g->nv * kGroupBytesPerVertex)
     s->group_min = 0;  // the batch state does not fit the memory budget
   s->timeout_ns = (uint64_t)(o && o->timeout_ms ? o->timeout_ms : 60000u) * 1000000ull;

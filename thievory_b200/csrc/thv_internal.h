@@ -76,6 +76,9 @@ struct Plan {
   char *d_lists = nullptr;
   uint32_t *d_list_idx = nullptr;
   uint64_t list_bytes = 0, list_vertices = 0, d_lists_bytes = 0;
+  // access tracking: link bytes per block (device counters) and the flags
+  uint32_t flags = 0;
+  unsigned long long *d_access = nullptr;
   // PageRank tiles (built lazily)
   bool tiles_valid = false;
   std::vector<PrTile> tiles;
@@ -126,6 +129,10 @@ struct thv_graph {
   uint64_t h_edges_dev = 0;       // device address of h_edges
   std::vector<uint32_t> outdeg;   // CSC only
   mutable std::vector<uint32_t> h_unpacked;  // {dst, w} view of packed edges
+  // link bytes recorded under earlier tracked plans, per vertex range
+  // (access_vb has one entry more than access_bytes)
+  std::vector<uint32_t> access_vb;
+  std::vector<uint64_t> access_bytes;
   // device
   cudaStream_t stream = nullptr;
   uint64_t *d_off = nullptr;
@@ -149,6 +156,7 @@ namespace thv {
 
 thv_status graph_init_device(thv_graph *g);  // stream, d_off, d_outdeg
 thv_status set_packing(thv_graph *g, bool on);  // weighted graphs only
+thv_status replan_by_access(thv_graph *g);      // THV_PLACE_ACCESS, same budget
 thv_status ensure_transpose(thv_graph *g, cudaStream_t st);  // transpose.cu
 thv_status convert_edge_list(const char *txt, const char *out_path, thv_format fmt,
                              uint32_t skip, uint32_t flags, int device, uint64_t *nv_out,
