@@ -47,7 +47,7 @@ FALLBACK_HBM_GBS = 6650.0
 NCU_TRAFFIC = {
     "sssp": dict(scale=22, ne=65241959, dram=600403968 + 87389440, sysmem=3375952 * 32),
     "cc": dict(scale=22, ne=128306542, dram=392704512 + 69563648, sysmem=11788847 * 32),
-    "bfs": dict(scale=20, ne=16084564, dram=78297088 + 4716544, sysmem=0),
+    "bfs": dict(scale=20, ne=16084564, dram=41359616 + 613888, sysmem=0),
     "pr_pull": dict(scale=22, ne=65241959, dram=135399168 + 20317184, sysmem=6104134 * 32, per="iteration"),
 }
 
