@@ -209,6 +209,27 @@ def algorithmic_bytes(off, vals, nv, vb, res, esz, algo, n_iters=1, list_deg=0):
     return hbm * n_iters, link * n_iters, int(d.sum())
 
 
+UF_SAMPLE = 2  # neighbours each vertex unions with first (union-find CC)
+
+
+def algorithmic_bytes_cc_uf(off, labels, nv, vb, res, esz, list_deg):
+    """Bytes sampling union-find CC must move on a symmetric graph: offsets
+    and label init/flatten per vertex (16 + 12 B), the first UF_SAMPLE
+    neighbours of every vertex and the rest of the lists of vertices outside
+    the highest-degree vertex's component, each edge with two 4 B label
+    probes; adjacency over the link where its block is on the host and the
+    list is not in the small-list cache."""
+    deg = np.diff(off.astype(np.int64))
+    hub = int(np.argmax(deg))
+    outside = labels != labels[hub]
+    edges_v = np.minimum(deg, UF_SAMPLE) + np.where(outside, np.maximum(deg - UF_SAMPLE, 0), 0)
+    blk = np.searchsorted(vb.astype(np.int64), np.arange(nv), side="right") - 1
+    resident_v = res[blk] | ((deg > 0) & (deg < list_deg))
+    link = int((edges_v[~resident_v] * esz).sum())
+    hbm = int((edges_v[resident_v] * esz).sum() + edges_v.sum() * 8 + nv * (16 + 12))
+    return hbm, link, int(edges_v.sum())
+
+
 def run_ours(args, dist):
     import torch
     import thievory_b200 as T
@@ -230,7 +251,8 @@ def run_ours(args, dist):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
     stream = torch.cuda.Stream(device=dev)
 
-    def measure(wl, k, w, want_e2e, want_cpu):
+    def measure(wl, k, w, want_e2e, want_cpu, run_kw=None):
+        run_kw = dict(run_kw or {})
         g = T.Graph.generate_rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"],
                                   fmt=wl["fmt"], device=dev)
         budget = wl.get("budget", int(wl.get("frac", 1.0) * g.ne * g.esz))
@@ -240,16 +262,20 @@ def run_ours(args, dist):
         src = args.source
         sptr = stream.cuda_stream
         for _ in range(w):
-            g.run(algo, source=src, want_values=False, stream=sptr)
+            g.run(algo, source=src, want_values=False, stream=sptr, **run_kw)
         vals = g.values(algo)
         off, edges, outdeg = g.host_arrays()
         vb, res = g.blocks()
         iters = 20 if algo.startswith("pr") else 1
         lcd = 0 if algo.startswith("pr") else plan["small_list_degree"]
-        b_hbm, b_link, trav = algorithmic_bytes(off, vals if algo in ("bfs", "sssp") else None,
-                                                g.nv, vb, res, g.mem_esz, algo, iters, lcd)
+        union_find = algo == "cc" and g.symmetric and not run_kw.get("label_propagation")
+        if union_find:
+            b_hbm, b_link, _ = algorithmic_bytes_cc_uf(off, vals, g.nv, vb, res, g.mem_esz, lcd)
+        else:
+            b_hbm, b_link, trav = algorithmic_bytes(off, vals if algo in ("bfs", "sssp") else None,
+                                                    g.nv, vb, res, g.mem_esz, algo, iters, lcd)
         if algo == "cc" or algo.startswith("pr"):
-            trav = g.ne * iters
+            trav = g.ne * iters  # edges of the graph, however many were read
         clocks = Clocks(dev)
         clocks.start()
         dist.barrier()
@@ -261,7 +287,7 @@ def run_ours(args, dist):
             for i in range(k):
                 flush.zero_()  # > L2 write between steps (outside the events)
                 ev[i][0].record(stream)
-                _, st = g.run(algo, source=src, want_values=False, stream=sptr)
+                _, st = g.run(algo, source=src, want_values=False, stream=sptr, **run_kw)
                 ev[i][1].record(stream)
                 lib_ms.append(st["device_ms"])
                 launches += st["kernel_launches"]
@@ -275,7 +301,8 @@ def run_ours(args, dist):
         value = dist.n * trav * k / total_s / 1e9
         t_roof = b_hbm / (hbm_peak * 1e9) + b_link / (link_peak * 1e9)
         kern_s = statistics.mean(lib_ms) / 1e3
-        dram_t, link_t = traffic_for(algo, wl["scale"], g.ne, iters)
+        # the captured CC kernel is label propagation's; union-find has its own
+        dram_t, link_t = traffic_for("cc_uf" if union_find else algo, wl["scale"], g.ne, iters)
         out = {
             "value": value, "ms_per_step": total_s * 1e3 / k, "traversed_edges": trav,
             "plan": plan, "clocks": ck, "gpu_launches": launches,
@@ -304,7 +331,7 @@ def run_ours(args, dist):
             wall = []
             for _ in range(k):
                 t0 = time.perf_counter()
-                _, st = g.run(algo, source=src, out=hv, stream=sptr)
+                _, st = g.run(algo, source=src, out=hv, stream=sptr, **run_kw)
                 wall.append(time.perf_counter() - t0)
             tw = dist.max(sum(wall))
             out["e2e"] = {"value": dist.n * trav * k / tw / 1e9, "unit": "GTEPS",
@@ -353,8 +380,14 @@ def run_ours(args, dist):
                      not args.no_cpu)
         extra["cc_rmat_sym_40pct"] = {k: cc[k] for k in ("value", "ms_per_step", "traversed_edges",
                                                           "roofline", "gpu_launches")}
+        extra["cc_rmat_sym_40pct"]["algorithm"] = ("sampling union-find (the graph is symmetric): "
+                                                   "same labels as min-label propagation")
         if "cpu_baseline" in cc:
             extra["cc_rmat_sym_40pct"]["cpu_baseline"] = cc["cpu_baseline"]
+        lp = measure(dict(WORKLOADS["c2cc"], scale=wl["scale"]), args.steps, args.warmup, False,
+                     False, {"label_propagation": True})
+        extra["cc_rmat_sym_40pct_label_propagation"] = {
+            k: lp[k] for k in ("value", "ms_per_step", "traversed_edges", "roofline", "gpu_launches")}
     return wl, main, extra
 
 

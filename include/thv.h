@@ -124,6 +124,8 @@ typedef struct thv_graph_info {
   uint32_t device, weighted;
   uint32_t mem_esz;     /* bytes per edge as stored (host and HBM): 4 when packed */
   uint32_t weight_bits; /* packed: low bits of an edge hold w - min weight; 0 = not packed */
+  uint32_t sorted;      /* every list ascending by neighbour id */
+  uint32_t symmetric;   /* marked symmetric (see thv_set_symmetric) */
 } thv_graph_info;
 thv_status thv_info(const thv_graph *g, thv_graph_info *out);
 /* Weighted graphs are stored packed by default: each {u32 dst, u32 w} pair
@@ -132,6 +134,11 @@ thv_status thv_info(const thv_graph *g, thv_graph_info *out);
  * packed = 0 restores {dst, w} pairs, 1 packs again.  Drops the plan;
  * no effect on unweighted graphs. */
 thv_status thv_set_edge_packing(thv_graph *g, int packed);
+/* Asserts (1) or withdraws (0) that every edge u->w has its reverse w->u.
+ * CC then runs as sampling union-find (THV_RUN_LABEL_PROPAGATION).
+ * On a graph that is not symmetric, CC with this set returns the labels of
+ * its weakly connected components instead of the reference's. */
+thv_status thv_set_symmetric(thv_graph *g, int symmetric);
 /* Host views of the graph (valid until thv_close); edges in the format's
  * layout ({dst, w} pairs for weighted graphs, unpacked on first use).
  * outdeg NULL unless CSC. */
@@ -224,6 +231,11 @@ typedef struct thv_run_opts {
  * levels over an in-edge transpose (built in HBM on first use) when the
  * frontier is large; this flag keeps every level top-down.  Same results. */
 #define THV_RUN_TOP_DOWN_ONLY 8u
+/* CC on a graph marked symmetric (thv_set_symmetric, or generated with
+ * symmetric = 1) runs as sampling union-find, which reads the first two
+ * neighbours of every vertex and the lists of vertices outside the largest
+ * component only; this flag keeps min-label propagation.  Same labels. */
+#define THV_RUN_LABEL_PROPAGATION 16u
 
 typedef struct thv_stats {
   double device_ms;         /* CUDA-event time of the traversal */

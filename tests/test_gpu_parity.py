@@ -347,3 +347,78 @@ def test_bfs_direction_optimising_symmetric_and_toys(T, O):
         plan(g, 1.0)
         got, _ = g.run("bfs", source=0, timeout_ms=20000)
         assert np.array_equal(got, O.bfs(t, 0))
+
+
+def _upper_edges(csr):
+    off = csr.off.astype(np.int64)
+    u = np.repeat(np.arange(csr.nv), np.diff(off))
+    return int((csr.adj.astype(np.int64) > u).sum())
+
+
+@pytest.mark.parametrize("frac", BUDGETS)
+def test_cc_union_find_on_symmetric_graphs(T, O, g14s, frac):
+    """Marked symmetric: CC runs as sampling union-find, reads far fewer
+    edges and returns the min-label fixed point."""
+    want = O.cc(g14s)
+    with engine_graph(T, g14s) as g:
+        assert g.sorted and not g.symmetric
+        plan(g, frac)
+        lp, st_lp = g.run("cc", timeout_ms=20000)
+        g.set_symmetric(True)
+        uf, st_uf = g.run("cc", timeout_ms=20000)
+        assert np.array_equal(lp, want) and np.array_equal(uf, want)
+        assert st_uf["edges_expanded"] < _upper_edges(g14s) < st_lp["edges_expanded"]
+        lp2, _ = g.run("cc", label_propagation=True, timeout_ms=20000)
+        assert np.array_equal(lp2, want)
+
+
+def test_cc_union_find_generated_weighted_and_unsorted(T, O):
+    # generated symmetric graphs are marked symmetric and sorted
+    g = T.Graph.generate_rmat(13, 8, symmetric=True, fmt="wcsr")
+    assert g.symmetric and g.sorted and g.mem_esz == 4
+    s = O.rmat(13, 8, symmetric=True, weighted=True)
+    g.plan(int(0.4 * g.ne * g.esz), block_bytes=BLOCK)
+    got, st = g.run("cc", timeout_ms=20000)
+    assert np.array_equal(got, O.cc(s)) and st["edges_expanded"] < _upper_edges(s)
+    g.close()
+    # unsorted lists: the sample is any two neighbours; labels stay exact
+    rng = np.random.default_rng(5)
+    sym = O.rmat(12, 8, symmetric=True)
+    adj = sym.adj.copy()
+    for v in range(sym.nv):
+        a, b = int(sym.off[v]), int(sym.off[v + 1])
+        adj[a:b] = rng.permutation(adj[a:b])
+    with T.Graph.from_arrays(sym.off, adj, "csr") as g2:
+        g2.set_symmetric(True)
+        assert not g2.sorted
+        g2.plan(int(0.4 * g2.ne * 4), block_bytes=BLOCK)
+        got, st = g2.run("cc", timeout_ms=20000)
+        assert np.array_equal(got, O.cc(sym))
+
+
+def test_cc_union_find_many_components_and_toys(T, O):
+    """Components of every size, isolated vertices and a hub outside the
+    largest component: the sampled hub component must not hide edges."""
+    rng = np.random.default_rng(9)
+    parts, base = [], 0
+    for size in [1, 2, 3, 50, 400, 3000, 1, 7]:
+        if size > 1:
+            n_e = size * 3
+            s = rng.integers(0, size, n_e) + base
+            d = rng.integers(0, size, n_e) + base
+            parts.append((s, d))
+        base += size
+    # a star whose centre (highest degree) is a small component of its own
+    hub = base
+    leaves = np.arange(base + 1, base + 120)
+    parts.append((np.full(len(leaves), hub), leaves))
+    base += 120
+    s = np.concatenate([p[0] for p in parts])
+    d = np.concatenate([p[1] for p in parts])
+    g = O.from_edges(base, s, d, symmetric=True)
+    with T.Graph.from_arrays(g.off, g.adj, "csr") as eg:
+        eg.set_symmetric(True)
+        for frac in (0.0, 1.0):
+            eg.plan(int(frac * eg.ne * 4), block_bytes=BLOCK)
+            got, _ = eg.run("cc", timeout_ms=20000)
+            assert np.array_equal(got, O.cc(g)), frac

@@ -81,7 +81,8 @@ class _GraphInfo(ctypes.Structure):
     _fields_ = [("nv", ctypes.c_uint64), ("ne", ctypes.c_uint64), ("fmt", ctypes.c_uint32),
                 ("esz", ctypes.c_uint32), ("device", ctypes.c_uint32),
                 ("weighted", ctypes.c_uint32), ("mem_esz", ctypes.c_uint32),
-                ("weight_bits", ctypes.c_uint32)]
+                ("weight_bits", ctypes.c_uint32), ("sorted", ctypes.c_uint32),
+                ("symmetric", ctypes.c_uint32)]
 
 
 class _RmatOpts(ctypes.Structure):
@@ -117,7 +118,7 @@ class _QueryStats(ctypes.Structure):
 # Every function include/thv.h declares (tests check the library exports them).
 ABI_FUNCTIONS = [
     "thv_open", "thv_from_arrays", "thv_generate_rmat", "thv_save", "thv_close",
-    "thv_info", "thv_set_edge_packing", "thv_convert", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_get_block_access", "thv_save_plan", "thv_load_plan", "thv_run",
+    "thv_info", "thv_set_edge_packing", "thv_set_symmetric", "thv_convert", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_get_block_access", "thv_save_plan", "thv_load_plan", "thv_run",
     "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
     "thv_pick_sources", "thv_bfs_noalloc", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
@@ -146,6 +147,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_close": ([P], I32),
         "thv_info": ([P, ctypes.POINTER(_GraphInfo)], I32),
         "thv_set_edge_packing": ([P, I32], I32),
+        "thv_set_symmetric": ([P, I32], I32),
         "thv_convert": ([ctypes.c_char_p, ctypes.c_char_p, U32, U32, U32, I32,
                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)], I32),
         "thv_host_arrays": ([P, pp, pp, pp], I32),
@@ -221,6 +223,13 @@ class Graph:
         # esz: the format's bytes per edge; mem_esz: as stored (4 when packed)
         self.esz, self.weighted, self.device = int(info.esz), bool(info.weighted), int(info.device)
         self.mem_esz, self.weight_bits = int(info.mem_esz), int(info.weight_bits)
+        self.sorted, self.symmetric = bool(info.sorted), bool(info.symmetric)
+
+    def set_symmetric(self, symmetric: bool = True) -> None:
+        """Assert that every edge has its reverse: CC then runs as sampling
+        union-find and skips most adjacency lists."""
+        _check(load_library().thv_set_symmetric(self._h, 1 if symmetric else 0), "thv_set_symmetric")
+        self._refresh()
 
     def set_edge_packing(self, packed: bool) -> None:
         """Store weighted edges packed in 4 bytes (default) or as {dst, w}
@@ -321,13 +330,14 @@ class Graph:
             out: Optional[np.ndarray] = None, want_values: bool = True, stream: int = 0,
             sssp_delta: int = 0, timeout_ms: int = 0, small_degree: int = 0,
             chunk_edges: int = 0, checksum: bool = False, compaction: str = "",
-            sssp_growth: int = 0, top_down_only: bool = False):
+            sssp_growth: int = 0, top_down_only: bool = False, label_propagation: bool = False):
         """Run algo; returns (values or None, stats dict).  compaction:
         "" (per-algorithm default), "scan" or "queue"; sssp_growth: SSSP
         window growth per advance (0 = default 8, 1 = fixed windows)."""
         lib = load_library()
         flags = ((1 if checksum else 0) | (2 if compaction == "scan" else 0)
-                 | (4 if compaction == "queue" else 0) | (8 if top_down_only else 0))
+                 | (4 if compaction == "queue" else 0) | (8 if top_down_only else 0)
+                 | (16 if label_propagation else 0))
         o = _RunOpts(source, pr_iters, pr_damping, sssp_delta, timeout_ms,
                      ctypes.c_void_p(stream) if stream else None, small_degree, chunk_edges,
                      flags, sssp_growth)

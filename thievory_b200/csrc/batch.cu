@@ -196,10 +196,11 @@ __device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t u, uintpt
         }
         const unsigned b0 = __ballot_sync(kFull, i0), b1 = __ballot_sync(kFull, i1);
         if (b0 | b1) {
-          best = warp_min(best);
+          // improving lanes lower the word's pending minimum themselves (one
+          // warp-wide atomic instead of a shuffle reduction)
+          if (i0 || i1) atomicMin(a.wmin + (w[q] >> 5), best);
           if (lane == 0) {
             atomicOr(a.front + w[q], (unsigned long long)b0 | ((unsigned long long)b1 << 32));
-            atomicMin(a.wmin + (w[q] >> 5), best);
             mark_pending<MS_SSSP>(a, w[q]);
           }
         }

@@ -155,7 +155,8 @@ static thv_status sort_unique(unsigned long long *&d0, unsigned long long *&d1,
 
 thv_status graph_adopt(uint64_t nv, uint64_t ne, thv_format fmt, uint32_t esz,
                        std::vector<uint64_t> &off, const void *d_edges,
-                       std::vector<uint32_t> &outdeg, int device, thv_graph **out);
+                       std::vector<uint32_t> &outdeg, bool symmetric, int device,
+                       thv_graph **out);
 
 thv_status generate_rmat(const thv_rmat_opts *o, thv_format fmt, int device,
                          thv_graph **out) {
@@ -234,7 +235,7 @@ thv_status generate_rmat(const thv_rmat_opts *o, thv_format fmt, int device,
   d_off = nullptr;
   if (e != cudaSuccess) { dev_free(d_edges); return fail(THV_ECUDA, "copy offsets"); }
   const thv_format gfmt = fmt;
-  s = graph_adopt(nv, ne, gfmt, esz, off, d_edges, outdeg, device, out);
+  s = graph_adopt(nv, ne, gfmt, esz, off, d_edges, outdeg, o->symmetric != 0, device, out);
   dev_free(d_edges);
   return s;
 }

@@ -145,6 +145,13 @@ static thv_status validate(thv_graph *g) {
   if (bad_at >= 0)
     return fail(THV_EFORMAT, "edge %lld has neighbour id >= n=%llu",
                 (long long)bad_at, (unsigned long long)nv);
+  // sorted lists (the converter's order) allow reading only part of a list
+  int64_t unsorted = 0;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : unsorted)
+  for (int64_t v = 0; v < (int64_t)nv; v++)
+    for (uint64_t i = g->off[v] + 1; i < g->off[v + 1]; i++)
+      unsorted += e[i * stride] < e[(i - 1) * stride];
+  g->sorted = unsorted == 0;
   return THV_OK;
 }
 
@@ -770,7 +777,7 @@ static thv_status from_arrays(uint64_t nv, uint64_t ne, const uint64_t *off,
 
 thv_status graph_adopt(uint64_t nv, uint64_t ne, thv_format fmt, uint32_t esz,
                        std::vector<uint64_t> &off, const void *d_edges,
-                       std::vector<uint32_t> &outdeg, int device,
+                       std::vector<uint32_t> &outdeg, bool symmetric, int device,
                        thv_graph **out) {
   std::unique_ptr<thv_graph, void (*)(thv_graph *)> g(new thv_graph(), graph_destroy);
   g->nv = nv;
@@ -778,6 +785,8 @@ thv_status graph_adopt(uint64_t nv, uint64_t ne, thv_format fmt, uint32_t esz,
   g->fmt = fmt;
   g->esz = esz;
   g->weighted = esz == 8;
+  g->sorted = true;  // the generator sorts by (src, dst)
+  g->symmetric = symmetric;
   g->device = device;
   g->off.swap(off);
   g->outdeg.swap(outdeg);
@@ -903,6 +912,8 @@ thv_status thv_info(const thv_graph *g, thv_graph_info *o) {
   o->weighted = g->weighted;
   o->mem_esz = g->esz;
   o->weight_bits = g->packed ? g->wshift : 0;
+  o->sorted = g->sorted;
+  o->symmetric = g->symmetric;
   return THV_OK;
 }
 
@@ -912,6 +923,12 @@ thv_status thv_convert(const char *txt_path, const char *out_path, thv_format fm
   THV_GUARD_BEGIN
   return convert_edge_list(txt_path, out_path, fmt, skip_lines, flags, device, nv_out, ne_out);
   THV_GUARD_END
+}
+
+thv_status thv_set_symmetric(thv_graph *g, int symmetric) {
+  if (!g) return fail(THV_EINVAL, "null graph");
+  g->symmetric = symmetric != 0;
+  return THV_OK;
 }
 
 thv_status thv_set_edge_packing(thv_graph *g, int packed) {

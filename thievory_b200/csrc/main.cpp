@@ -38,6 +38,7 @@ static void usage(const char *prog) {
   printf("  --hbm-budget : resident edge bytes (e.g. 2G, 40%%; default: all that fit)\n");
   printf("  --block-bytes : edge block size (default 64M)\n");
   printf("  --placement : densest|prefix (default densest)\n");
+  printf("  --symmetric : 1 = the graph has every reverse edge (CC by union-find)\n");
   printf("  --pr-iters : PageRank iterations (default 20)\n");
   printf("  --values : output path (default results/values.bin)\n");
 }
@@ -66,7 +67,7 @@ int main(int argc, char **argv) {
   std::string values_path = "results/values.bin";
   unsigned edge_size = 4, source = 1, runs = 1, gpus = 0, pr_iters = 20;
   int device = 0;
-  bool has_input = false;
+  bool has_input = false, symmetric = false;
   for (int i = 1; i + 1 < argc; i += 2) {
     const char *k = argv[i], *v = argv[i + 1];
     if (!strcmp(k, "--input")) { input = v; has_input = true; }
@@ -82,6 +83,7 @@ int main(int argc, char **argv) {
     else if (!strcmp(k, "--placement")) placement = v;
     else if (!strcmp(k, "--pr-iters")) pr_iters = (unsigned)atoi(v);
     else if (!strcmp(k, "--values")) values_path = v;
+    else if (!strcmp(k, "--symmetric")) symmetric = atoi(v) != 0;
     else { fprintf(stderr, "Error: unknown flag %s\n", k); usage(argv[0]); return 1; }
   }
   if (!has_input) { usage(argv[0]); return 0; }
@@ -118,6 +120,7 @@ int main(int argc, char **argv) {
   thv_graph *g = nullptr;
   thv_status s = thv_open(input.c_str(), fmt, flags, device, &g);
   if (s != THV_OK) return die("open", s);
+  if (symmetric) thv_set_symmetric(g, 1);  // CC: sampling union-find
   thv_graph_info info{};
   thv_info(g, &info);
   printf("Num Vertices: %llu\n", (unsigned long long)info.nv);

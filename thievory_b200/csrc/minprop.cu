@@ -959,6 +959,251 @@ __global__ void values_checksum_kernel(const uint32_t *val, uint64_t nv,
   }
 }
 
+// ============================================= union-find CC (symmetric)
+//
+// On a symmetric graph the min-label fixed point is the smallest id of each
+// connected component, which union-find reaches without reading most of the
+// adjacency (the sampling scheme of Afforest, Sutton et al., IPDPS'18):
+//   1. every vertex unions with its first kUfSample neighbours;
+//   2. flatten; c = the component of the highest-degree vertex;
+//   3. every vertex outside c unions with the rest of its list; vertices in
+//      c skip theirs -- an edge with both ends in c changes nothing, and an
+//      edge with one end outside c is read from that end (its reverse is in
+//      the other end's list);
+//   4. flatten.
+// Roots are hooked larger-under-smaller with a CAS, so a parent id never
+// exceeds its child's and each root is its component's minimum id; finds
+// shortcut the path as they climb.
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t *p, uint32_t x) {
+  uint32_t cur = ldcg(p + x);
+  if (cur == x) return x;
+  uint32_t prev = x, next;
+  while (cur > (next = ldcg(p + cur))) {
+    p[prev] = next;  // shortcut to an ancestor: benign under races
+    prev = cur;
+    cur = next;
+  }
+  return cur;
+}
+
+__device__ __forceinline__ void uf_union(uint32_t *p, uint32_t u, uint32_t w) {
+  uint32_t ru = uf_find(p, u), rw = uf_find(p, w);
+  while (ru != rw) {
+    const uint32_t hi = max(ru, rw), lo = min(ru, rw);
+    const uint32_t old = atomicCAS(p + hi, hi, lo);
+    if (old == hi) return;  // hooked
+    // hi stopped being a root meanwhile: continue from the current roots
+    ru = uf_find(p, old);
+    rw = uf_find(p, lo);
+  }
+}
+
+constexpr uint32_t kUfSample = 2;
+
+// Step 1: each vertex (one thread) unions with its first kUfSample
+// neighbours.  (Storing the smallest neighbour as the parent outright, with
+// no CAS, measured slower: the parent chains it builds are long, and every
+// later find climbs them.)
+template <int ESZ>
+__device__ __forceinline__ void uf_sample_edges(const MinArgs &a, const uint32_t *vb,
+                                                const unsigned long long *bbase, uint32_t v,
+                                                uint32_t (&w)[kUfSample], uint32_t &k, bool &host) {
+  const uint64_t s = __ldg(a.off + v), e = __ldg(a.off + v + 1);
+  const uint32_t deg = (uint32_t)(e - s);
+  k = min(deg, kUfSample);
+  host = false;
+  if (!k) return;
+  const unsigned long long eaddr =
+      list_addr(a.lc, bbase[find_block(vb, a.nblk, v)], a.host_base, v, s, deg, ESZ, &host);
+#pragma unroll
+  for (uint32_t j = 0; j < kUfSample; j++) {
+    const uint32_t raw = j < k ? ld_nc_u32(eaddr + (unsigned long long)j * ESZ) : v;
+    w[j] = ESZ == 4 ? edge_dst(raw, a.wshift) : raw;
+  }
+}
+
+// block table of the plan in shared memory (as minprop_kernel stages it)
+#define UF_STAGE_BLOCKS()                                                                        \
+  extern __shared__ unsigned long long s_tab[];                                                 \
+  const bool smem_tab = a.nblk <= kSmemBlocks;                                                   \
+  unsigned long long *s_base = s_tab;                                                            \
+  uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_tab + a.nblk);                                 \
+  if (smem_tab) {                                                                                \
+    for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x) s_vb[i] = a.blk_vb[i];          \
+    for (uint32_t i = threadIdx.x; i < a.nblk; i += blockDim.x) s_base[i] = a.blk_base[i];       \
+  }                                                                                              \
+  __syncthreads();                                                                               \
+  const uint32_t *vb = smem_tab ? s_vb : a.blk_vb;                                               \
+  const unsigned long long *bbase = smem_tab ? s_base : (const unsigned long long *)a.blk_base;
+
+template <int ESZ>
+__global__ void __launch_bounds__(256) uf_sample(MinArgs a) {
+  UF_STAGE_BLOCKS();
+  unsigned long long my_edges = 0, my_hbm = 0, my_link = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nv; v += gridDim.x * blockDim.x) {
+    uint32_t w[kUfSample], k;
+    bool host;
+    uf_sample_edges<ESZ>(a, vb, bbase, v, w, k, host);
+    if (!k) continue;
+#pragma unroll
+    for (uint32_t j = 0; j < kUfSample; j++)
+      if (j < k && w[j] != v) uf_union(a.val, v, w[j]);
+    my_edges += k;
+    if (host) my_link += (unsigned long long)k * ESZ;
+    else my_hbm += (unsigned long long)k * ESZ;
+  }
+  my_edges = warp_sum(my_edges);
+  my_hbm = warp_sum(my_hbm);
+  my_link = warp_sum(my_link);
+  if (lane_id() == 0 && my_edges) {
+    atomicAdd(&a.ctrl->edges, my_edges);
+    atomicAdd(&a.ctrl->hbm_bytes, my_hbm);
+    atomicAdd(&a.ctrl->link_bytes, my_link);
+  }
+}
+
+// Step 3 work items: the lists past the sample of every vertex outside the
+// component of `hub` (labels are flattened roots here).
+template <int ESZ>
+__global__ void __launch_bounds__(256) uf_items(MinArgs a, uint32_t hub) {
+  const uint32_t skip = ldcg(a.val + hub);
+  MinCtrl *c = a.ctrl;
+  const unsigned lane = lane_id();
+  const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t nwords = (a.nv + 31) / 32;
+  unsigned long long my_edges = 0, my_hbm = 0, my_link = 0;
+  for (uint32_t word = gwarp; word < nwords; word += nwarps) {
+    const uint32_t v = word * 32u + lane;
+    uint32_t cnt = 0;
+    unsigned long long eaddr = 0;
+    if (v < a.nv && ldcg(a.val + v) != skip) {
+      const uint64_t s = __ldg(a.off + v), e = __ldg(a.off + v + 1);
+      const uint32_t deg = (uint32_t)(e - s);
+      if (deg > kUfSample) {
+        bool host;
+        eaddr = list_addr(a.lc, __ldg(a.blk_base + find_block(a.blk_vb, a.nblk, v)), a.host_base,
+                          v, s, deg, ESZ, &host);
+        cnt = deg - kUfSample;
+        eaddr += (unsigned long long)kUfSample * ESZ;
+        my_edges += cnt;
+        if (host) my_link += (unsigned long long)cnt * ESZ;
+        else my_hbm += (unsigned long long)cnt * ESZ;
+      }
+    }
+    const bool small = cnt > 0 && cnt < a.small_deg;
+    const bool big = cnt >= a.small_deg;
+    const unsigned sm = __ballot_sync(kFull, small);
+    if (sm) {
+      const int ldr = __ffs(sm) - 1;
+      unsigned long long base = 0;
+      if (lane == (unsigned)ldr) base = atomicAdd(&c->cnt_small[0], (unsigned long long)__popc(sm));
+      base = shfl64(base, ldr);
+      const unsigned long long pos = base + __popc(sm & lanemask_lt());
+      if (small) {
+        if (pos < a.cap_s) a.qs[pos] = make_item(eaddr, cnt, v, v);
+        else atomicCAS(&c->err, 0u, kDevErrQueue);
+      }
+    }
+    if (__any_sync(kFull, big)) {
+      const unsigned nch = big ? (cnt + a.chunk - 1) / a.chunk : 0u;
+      const unsigned inc = warp_incl_scan<unsigned>(nch);
+      const unsigned tot = __shfl_sync(kFull, inc, 31);
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&c->cnt_big[0], (unsigned long long)tot);
+      base = shfl64(base, 0);
+      if (big) {
+        unsigned long long pos = base + inc - nch;
+        for (unsigned k = 0; k < nch; k++, pos++) {
+          const uint32_t lo = k * a.chunk;
+          if (pos < a.cap_b)
+            a.qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, min(a.chunk, cnt - lo), v, v);
+          else
+            atomicCAS(&c->err, 0u, kDevErrQueue);
+        }
+      }
+    }
+  }
+  my_edges = warp_sum(my_edges);
+  my_hbm = warp_sum(my_hbm);
+  my_link = warp_sum(my_link);
+  if (lane == 0 && my_edges) {
+    atomicAdd(&c->edges, my_edges);
+    atomicAdd(&c->hbm_bytes, my_hbm);
+    atomicAdd(&c->link_bytes, my_link);
+  }
+}
+
+template <int ESZ>
+__global__ void __launch_bounds__(256) uf_unions(MinArgs a) {
+  MinCtrl *c = a.ctrl;
+  const unsigned lane = lane_id();
+  const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  const unsigned long long ns = min(ldcg(&c->cnt_small[0]), a.cap_s);
+  const unsigned long long nb = min(ldcg(&c->cnt_big[0]), a.cap_b);
+  const unsigned long long ntask = nb + (ns + 31) / 32;
+  constexpr int PER = 16 / ESZ;
+  for (unsigned long long t = gwarp; t < ntask; t += nwarps) {
+    if (t < nb) {
+      // a chunk of one list: 16-byte loads, lanes outside [start, end) masked
+      const MinItem it = a.qb[t];
+      const uintptr_t start = it.ea_cnt & kAddrMask;
+      const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
+      for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end; p += 512u) {
+        const uint4 q = ld_nc_v4(p);
+        const uint32_t f[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+          const uintptr_t ea = p + (uintptr_t)ESZ * j;
+          if (ea >= start && ea < end)
+            uf_union(a.val, it.v, ESZ == 4 ? edge_dst(f[j], a.wshift) : f[2 * j]);
+        }
+      }
+    } else {
+      // 32 short suffixes, their edges spread over the lanes
+      const unsigned long long idx = (t - nb) * 32ull + lane;
+      MinItem it{0, 0, 0};
+      if (idx < ns) it = a.qs[idx];
+      const unsigned cnt = (unsigned)(it.ea_cnt >> 48);
+      const unsigned long long eaddr = it.ea_cnt & kAddrMask;
+      const unsigned incl = warp_incl_scan<unsigned>(cnt);
+      const unsigned excl = incl - cnt;
+      const unsigned total = __shfl_sync(kFull, incl, 31);
+      for (unsigned k = 0; k < total; k += 32) {
+        const unsigned tt = k + lane;
+        const int o = warp_owner(excl, tt);
+        const unsigned long long ea = shfl64(eaddr, o);
+        const unsigned oex = __shfl_sync(kFull, excl, o);
+        const uint32_t ou = __shfl_sync(kFull, it.v, o);
+        if (tt < total) {
+          const uint32_t raw = ld_nc_u32((uintptr_t)ea + (uintptr_t)(tt - oex) * ESZ);
+          uf_union(a.val, ou, ESZ == 4 ? edge_dst(raw, a.wshift) : raw);
+        }
+      }
+    }
+  }
+}
+
+__global__ void uf_flatten(uint32_t *p, uint32_t nv) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
+    uint32_t r = ldcg(p + v);
+    while (true) {
+      const uint32_t n = ldcg(p + r);
+      if (n == r) break;
+      r = n;
+    }
+    p[v] = r;
+  }
+}
+
+__global__ void uf_init(MinArgs a) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < a.nv; v += gridDim.x * blockDim.x)
+    a.val[v] = v;
+  if (blockIdx.x == 0 && threadIdx.x == 0) memset(a.ctrl, 0, sizeof(MinCtrl));
+}
+
 // ------------------------------------------------------------------ host --
 
 static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
@@ -1122,7 +1367,30 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   uint32_t launches = 0;
   THV_CUDA(cudaEventRecord(ms->ev0, st));
   thv_status s = THV_OK;
-  if (g->esz == 4) {
+  // CC of a symmetric graph: sampling union-find (same labels as min-label
+  // propagation, most lists never read)
+  const bool union_find = op == OP_CC && g->symmetric && g->nv > 0 &&
+                          !(o && (o->flags & THV_RUN_LABEL_PROPAGATION));
+  if (union_find) {
+    const int grid = g->num_sms * 8;
+    const uint32_t hub = g->hub_vertex();
+    const size_t nb = g->plan.blocks.size();
+    const size_t smem = nb <= kSmemBlocks ? nb * 8 + (nb + 1) * 4 : 0;
+    uf_init<<<grid, 256, 0, st>>>(a);
+    if (g->esz == 4) uf_sample<4><<<grid, 256, smem, st>>>(a);
+    else uf_sample<8><<<grid, 256, smem, st>>>(a);
+    uf_flatten<<<grid, 256, 0, st>>>(a.val, a.nv);
+    if (g->esz == 4) {
+      uf_items<4><<<grid, 256, 0, st>>>(a, hub);
+      uf_unions<4><<<grid, 256, 0, st>>>(a);
+    } else {
+      uf_items<8><<<grid, 256, 0, st>>>(a, hub);
+      uf_unions<8><<<grid, 256, 0, st>>>(a);
+    }
+    uf_flatten<<<grid, 256, 0, st>>>(a.val, a.nv);
+    THV_CUDA(cudaGetLastError());
+    launches += 6;
+  } else if (g->esz == 4) {
     if (op == OP_BFS) s = launch_minprop<OP_BFS, 4>(g, a, st, launches, scan_mode);
     else if (op == OP_CC) s = launch_minprop<OP_CC, 4>(g, a, st, launches, scan_mode);
     else s = launch_minprop<OP_SSSP, 4>(g, a, st, launches, scan_mode);  // packed weights

@@ -118,6 +118,17 @@ struct thv_graph {
   thv_format fmt = THV_FMT_CSR;
   uint32_t esz = 4;       // bytes per edge in memory (host and HBM copies)
   bool weighted = false;
+  bool sorted = false;     // every adjacency list ascending by neighbour id
+  bool symmetric = false;  // every u->w has w->u (asserted or by construction)
+  int64_t hub = -1;        // a vertex of maximum out-degree (lazily found)
+  uint32_t hub_vertex() {
+    if (hub < 0) {
+      hub = 0;
+      for (uint64_t v = 1; v < nv; v++)
+        if (off[v + 1] - off[v] > off[hub + 1] - off[hub]) hub = (int64_t)v;
+    }
+    return (uint32_t)hub;
+  }
   // packed weighted edges: 4 bytes = dst << wshift | (w - wbase)
   bool packed = false;
   uint32_t wshift = 0, wbase = 0;
