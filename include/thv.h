@@ -379,6 +379,11 @@ uint32_t thv_abi_version(void);
 /* Host fault injection for tests: the n-th subsequent pinned/device
  * allocation made by the library fails (0 disables). */
 void thv_debug_fail_alloc_after(uint32_t n);
+/* Failure detection without a fault: a two-block launch in which one block
+ * never reaches the grid barrier, so the other's bounded wait runs out after
+ * timeout_ms (1..10000) and records the error the traversals report.
+ * Returns THV_ETIMEOUT; the context stays usable. */
+thv_status thv_debug_wait_timeout(int device, uint32_t timeout_ms);
 
 #ifdef __cplusplus
 }

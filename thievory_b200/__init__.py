@@ -122,7 +122,7 @@ ABI_FUNCTIONS = [
     "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
     "thv_pick_sources", "thv_bfs_noalloc", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
-    "thv_debug_fail_alloc_after",
+    "thv_debug_fail_alloc_after", "thv_debug_wait_timeout",
 ]
 
 _lib = None
@@ -174,6 +174,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_status_str": ([I32], ctypes.c_char_p),
         "thv_abi_version": ([], U32),
         "thv_debug_fail_alloc_after": ([U32], None),
+        "thv_debug_wait_timeout": ([I32, U32], I32),
     }
     for name, (argt, rest) in sig.items():
         fn = getattr(lib, name)

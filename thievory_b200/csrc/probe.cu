@@ -1,6 +1,7 @@
 // Host-link bandwidth probe: the denominator for zero-copy edge reads.
 #include <algorithm>
 #include <cstring>
+#include <exception>
 
 #include "thv_device.cuh"
 #include "thv_internal.h"
@@ -69,5 +70,48 @@ extern "C" thv_status thv_link_bandwidth(int device, uint64_t bytes, double *mem
     return thv::measure(device, bytes, memcpy_gbs, zerocopy_gbs);
   } catch (...) {
     return thv::fail(THV_EINVAL, "exception in link probe");
+  }
+}
+
+// ---------------------------------------------------------- wait timeout --
+// Block 0 leaves without reaching the grid barrier, so block 1's bounded
+// wait runs out after timeout_ns and records the barrier error: the path a
+// traversal takes when a block stops making progress, exercised without a
+// fault (the wait is limited by %globaltimer and always ends).
+namespace thv {
+
+__global__ void wait_timeout_probe(GridBar *bar, unsigned *err, unsigned long long timeout_ns) {
+  if (blockIdx.x == 0) return;
+  grid_sync(bar, err, timeout_ns);
+}
+
+}  // namespace thv
+
+extern "C" thv_status thv_debug_wait_timeout(int device, uint32_t timeout_ms) {
+  using namespace thv;
+  try {
+    if (timeout_ms == 0 || timeout_ms > 10000) return fail(THV_EINVAL, "timeout must be 1..10000 ms");
+    THV_CUDA(cudaSetDevice(device));
+    struct Scratch {
+      GridBar bar;
+      unsigned err, pad;
+    };
+    Scratch *d = nullptr;
+    THV_TRY(dev_alloc((void **)&d, sizeof(Scratch), "wait probe"));
+    Scratch h{};
+    thv_status s = THV_OK;
+    if (cudaMemset(d, 0, sizeof(Scratch)) != cudaSuccess) s = fail(THV_ECUDA, "memset");
+    if (s == THV_OK) {
+      wait_timeout_probe<<<2, 32>>>(&d->bar, &d->err, (unsigned long long)timeout_ms * 1000000ull);
+      if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+          cudaMemcpy(&h, d, sizeof(Scratch), cudaMemcpyDeviceToHost) != cudaSuccess)
+        s = fail(THV_ECUDA, "wait probe launch failed");
+    }
+    dev_free(d);
+    if (s != THV_OK) return s;
+    if (h.err == kDevErrBarrier) return fail(THV_ETIMEOUT, "grid barrier wait exceeded %u ms", timeout_ms);
+    return fail(THV_EDEVICE, "wait probe ended without a timeout (error word %u)", h.err);
+  } catch (const std::exception &e) {
+    return fail(THV_ECUDA, "wait probe: %s", e.what());
   }
 }
