@@ -302,10 +302,13 @@ typedef struct thv_serve_opts {
   uint32_t timeout_ms;       /* bound on device waits; 0 = 60000 */
   uint32_t max_batch_iters;  /* iterations per launch while requests wait;
                                 0 = 4 */
-  uint32_t group_min;        /* queue depth from which waiting queries run
-                                as batched groups of up to 64 (the
-                                thv_batch_run kernels) instead of slots;
-                                0 = 2, 0xFFFFFFFF = never (slots only) */
+  uint32_t group_min;        /* batching: whenever the device is free, up
+                                to 64 waiting queries of the front query's
+                                algorithm run as one batched group (the
+                                thv_batch_run kernels) if at least group_min
+                                of them wait, else the front query runs
+                                alone; 0 = measured defaults (BFS 4, SSSP
+                                6); 0xFFFFFFFF = no batching (slots) */
   uint32_t replan_every;     /* re-place the graph's blocks by measured
                                 access (THV_PLACE_ACCESS, same budget) after
                                 this many finished queries; 0 = never */

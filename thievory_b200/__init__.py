@@ -424,8 +424,9 @@ class Server:
     def __init__(self, graph: Graph, max_slots: int = 64, queue_capacity: int = 0,
                  mem_budget_bytes: int = 0, timeout_ms: int = 0, max_batch_iters: int = 0,
                  group_min: int = 0, replan_every: int = 0):
-        """group_min: queue depth from which waiting queries run as batched
-        groups (0 = 2, 0xFFFFFFFF = never: slots only)."""
+        """group_min: waiting queries of one algorithm that run as a batched
+        group (0 = measured defaults: BFS 4, SSSP 6; 0xFFFFFFFF = no
+        batching: slot admission)."""
         lib = load_library()
         self.graph = graph
         self._bufs = {}

@@ -481,10 +481,11 @@ struct Query {
 // Batched-group mode: device bytes per vertex of the batch state (masks,
 // 64 distance or level columns, 64-column output staging, queues).
 constexpr uint64_t kGroupBytesPerVertex = 600;
-// Measured at RMAT-26 (47% HBM, 80% BFS / 20% SSSP Poisson stream): with
-// groups from 2 waiting queries the server beats slot admission at every
-// load (19.5 q/s offered: p50 61 vs 157 ms; 1245 q/s: 192 vs 165 q/s).
-constexpr uint32_t kDefaultGroupMin = 2;
+// Smallest group worth a batched launch, per algorithm: below it the waiting
+// queries run one after another on the single-source kernel.  RMAT-26, 47%
+// HBM: a batched group of k BFS sources beats k single runs from k = 4
+// (1.16x; 3: 0.91x), of k SSSP sources from k = 6 (1.17x; 4: 0.90x).
+constexpr uint32_t kGroupMinBfs = 4, kGroupMinSssp = 6;
 constexpr uint32_t kGroupMax = 64;
 
 }  // namespace
@@ -492,7 +493,8 @@ constexpr uint32_t kGroupMax = 64;
 struct thv_server {
   thv_graph *g = nullptr;
   uint32_t W = 0, queue_cap = 0, batch_iters = 4;
-  uint32_t group_min = 0;  // 0: group mode off
+  bool batching = true;    // batched groups + lone runs (false: slots)
+  uint32_t group_min = 0;  // explicit group threshold; 0 = per algorithm
   uint32_t replan_every = 0;        // queries between access re-placements
   uint64_t done_since_replan = 0;
   uint64_t timeout_ns = 0;
@@ -760,24 +762,41 @@ void worker_loop(thv_server *s) {
       // A deep queue runs as batched groups: stop admitting into slots, and
       // once the slots have drained take up to 64 waiting queries of the
       // front query's algorithm (FIFO within that algorithm).
-      const bool deep = s->group_min && s->waiting.size() >= s->group_min;
-      if (deep && !s->active) {
+      // Batching: whenever the device is free, the front query's algorithm
+      // runs as one batched group of up to 64 waiting queries if enough of
+      // them wait, else the front query runs alone on the single-source
+      // kernel.  Without batching: lone runs when one query waits, slots
+      // (admission into the running traversal) otherwise.
+      const bool deep = s->batching;
+      if (s->batching && !s->active && !s->waiting.empty()) {
         galgo = s->queries[s->waiting.front()].algo;
-        for (auto it = s->waiting.begin(); it != s->waiting.end() && group.size() < kGroupMax;) {
-          if (s->queries[*it].algo == galgo) {
-            group.push_back(*it);
-            it = s->waiting.erase(it);
-          } else {
-            ++it;
+        uint32_t k = 0;
+        for (uint64_t t : s->waiting) k += s->queries[t].algo == galgo;
+        const uint32_t kmin = s->group_min ? s->group_min
+                                           : (galgo == THV_ALGO_BFS ? kGroupMinBfs : kGroupMinSssp);
+        if (k >= kmin) {
+          for (auto it = s->waiting.begin(); it != s->waiting.end() && group.size() < kGroupMax;) {
+            if (s->queries[*it].algo == galgo) {
+              group.push_back(*it);
+              it = s->waiting.erase(it);
+            } else {
+              ++it;
+            }
           }
+          const double now = clock_ms();
+          for (uint64_t t : group) {
+            Query &q = s->queries[t];
+            q.t_start = now;
+            q.mode = 1;
+          }
+        } else {
+          group.push_back(s->waiting.front());
+          s->waiting.pop_front();
+          Query &q = s->queries[group[0]];
+          q.t_start = clock_ms();
+          q.mode = 2;
         }
-        const double now = clock_ms();
-        for (uint64_t t : group) {
-          Query &q = s->queries[t];
-          q.t_start = now;
-          q.mode = 1;
-        }
-      } else if (!deep && !s->active && s->waiting.size() == 1) {
+      } else if (!s->batching && !s->active && s->waiting.size() == 1) {
         // an idle server with one request: the single-source kernel
         group.push_back(s->waiting.front());
         s->waiting.pop_front();
@@ -864,11 +883,11 @@ thv_status start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
   s->W = W;
   s->queue_cap = o && o->queue_capacity ? o->queue_capacity : 65536u;
   s->batch_iters = o && o->max_batch_iters ? o->max_batch_iters : 4u;
-  s->group_min = o && o->group_min ? (o->group_min == 0xFFFFFFFFu ? 0u : o->group_min)
-                                   : kDefaultGroupMin;
+  s->batching = !(o && o->group_min == 0xFFFFFFFFu);
+  s->group_min = o && o->group_min && o->group_min != 0xFFFFFFFFu ? o->group_min : 0u;
   s->replan_every = o ? o->replan_every : 0;
   if (o && o->mem_budget_bytes && o->mem_budget_bytes < g->nv * kGroupBytesPerVertex)
-    s->group_min = 0;  // the batch state does not fit the memory budget
+    s->batching = false;  // the batch state does not fit the memory budget
   s->timeout_ns = (uint64_t)(o && o->timeout_ms ? o->timeout_ms : 60000u) * 1000000ull;
   const uint64_t nw = (g->nv + 31) / 32;
   s->ngroups = (uint32_t)((nw + 31) / 32);
