@@ -12,8 +12,9 @@
 //        u->w with frontier mask f does m = f & ~visit[w]; atomicOr(visit[w],
 //        m) hands each newly reached (w, s) to exactly one thread, which
 //        writes level byte lvl[w][s] = iteration + 1 and marks w pending.
-//   SSSP dist[w][s] rows of 64 u32 (vertex-major, one 256-byte row per
-//        vertex); per edge and source in the mask the single-source
+//   SSSP dist[w][.] rows of 64 u32 (vertex-major, one 256-byte row per
+//        vertex; source s at word row_pos(s)); per edge and source in the
+//        mask the single-source
 //        relaxation "cand < dist => atomicMin, mark pending" with the same
 //        near/far window, shared by all sources.
 // Results are bit-identical to single-source runs: BFS levels are exact
@@ -38,6 +39,16 @@ constexpr uint32_t kMsWidth = 64;       // sources per group (mask bits)
 constexpr uint32_t kMaxBfsLevel = 254;  // u8 level bytes hold level + 1
 constexpr uint32_t kMsGrowth = 1;       // SSSP window width factor per advance
 constexpr uint32_t kMsDelta = 256;      // SSSP window width shared by a group
+// SSSP: distance-row loads per lane in flight (two edges each); more spill
+// registers at 64 per thread and run slower
+constexpr int kMsRowsInFlight = 4;
+
+// Word of source s in a 64-word SSSP distance row: lane l of a half-warp
+// holds sources l, l+16, l+32, l+48 as one 16-byte word group (4l..4l+3),
+// so one 16-byte load per lane reads a whole row per half-warp.
+__host__ __device__ __forceinline__ uint32_t row_pos(uint32_t s) {
+  return 4u * (s & 15u) + (s >> 4);
+}
 
 struct MsCtrl {
   GridBar bar;
@@ -118,7 +129,11 @@ __device__ __forceinline__ void ms_bfs_edge(const MsArgs &a, uint32_t w,
   }
 }
 
-// SSSP edge u->w of weight wt for the sources in f.
+// SSSP edge u->w of weight wt for the sources in f.  The distance update
+// is a fire-and-forget atomicMin: when cand is below the value read, (w, s)
+// is marked pending whether this lane or a concurrent one ends up lowering
+// dist[w][s] (the lower writer marks the same bit in the same phase), so
+// the lane never waits for the old value.
 __device__ __forceinline__ void ms_sssp_edge(const MsArgs &a, uint32_t u, uint32_t w,
                                              uint32_t wt, unsigned long long f) {
   const uint32_t *du = a.dist + (size_t)u * kMsWidth;
@@ -128,13 +143,12 @@ __device__ __forceinline__ void ms_sssp_edge(const MsArgs &a, uint32_t u, uint32
   while (f) {
     const int s = __ffsll((long long)f) - 1;
     f &= f - 1;
-    const unsigned long long cand = (unsigned long long)ldcg(du + s) + wt;
-    if (cand < ldcg(dw + s)) {
-      const uint32_t old = atomicMin(dw + s, (uint32_t)cand);
-      if (cand < old) {
-        improved |= 1ull << s;
-        best = min(best, (uint32_t)cand);
-      }
+    const uint32_t p = row_pos((uint32_t)s);
+    const unsigned long long cand = (unsigned long long)ldcg(du + p) + wt;
+    if (cand < ldcg(dw + p)) {
+      atomicMin(dw + p, (uint32_t)cand);
+      improved |= 1ull << s;
+      best = min(best, (uint32_t)cand);
     }
   }
   if (improved) {
@@ -144,64 +158,81 @@ __device__ __forceinline__ void ms_sssp_edge(const MsArgs &a, uint32_t u, uint32
   }
 }
 
-// Lane-per-source SSSP relaxation of one work item: the warp loads the
-// item's edges 32 at a time (coalesced) and relaxes each edge for every
-// source of the mask at once, lanes = sources, so dist[w][.] is read as
-// coalesced 128-byte lines; four edges' rows are in flight per step.
+// Half-warp-per-edge SSSP relaxation of one work item: the warp loads the
+// item's edges 32 at a time (coalesced); each half-warp takes one edge and
+// reads its whole 256-byte distance row with one 16-byte load per lane
+// (lane l: sources l, l+16, l+32, l+48), so a warp step relaxes two edges
+// for all 64 sources and four steps (eight edges) have their rows in
+// flight together.  Distance updates are fire-and-forget as in
+// ms_sssp_edge; four ballots give each edge's improved-source mask.
 template <int ESZ>
 __device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t u, uintptr_t eaddr,
                                              uint32_t cnt, unsigned long long f) {
-  const unsigned lane = lane_id();
-  const bool lo = (f >> lane) & 1ull, hi = (f >> (lane + 32)) & 1ull;
-  const uint32_t *du = a.dist + (size_t)u * kMsWidth;
-  const uint32_t d0 = lo ? ldcg(du + lane) : 0u, d1 = hi ? ldcg(du + 32 + lane) : 0u;
-  for (uint32_t base = 0; base < cnt; base += 32) {
-    const uint32_t k = base + lane;
-    uint2 e = make_uint2(0, 0);
+  const unsigned lane = lane_id(), hl = lane & 15u, half = lane >> 4;
+  const uint32_t mb = (uint32_t)((f >> hl) & 1ull) | (uint32_t)((f >> (hl + 15u)) & 2ull) |
+                      (uint32_t)((f >> (hl + 30u)) & 4ull) | (uint32_t)((f >> (hl + 45u)) & 8ull);
+  uint4 du4 = make_uint4(0, 0, 0, 0);
+  if (mb) du4 = __ldcg(reinterpret_cast<const uint4 *>(a.dist + (size_t)u * kMsWidth) + hl);
+  const uint32_t du[4] = {du4.x, du4.y, du4.z, du4.w};
+  // packed edges stay raw until used (one register per edge in flight)
+  auto load_edge = [&](uint32_t k) {
+    uint2 r = make_uint2(0, 0);
     if (k < cnt) {
-      if (ESZ == 8) {
-        e = ld_nc_u2(eaddr + (uintptr_t)k * 8u);
-      } else {
-        const uint32_t r = ld_nc_u32(eaddr + (uintptr_t)k * 4u);
-        e = make_uint2(edge_dst(r, a.wshift), edge_wt(r, a.wshift, a.wbase));
-      }
+      if (ESZ == 8) r = ld_nc_u2(eaddr + (uintptr_t)k * 8u);
+      else r.x = ld_nc_u32(eaddr + (uintptr_t)k * 4u);
     }
+    return r;
+  };
+  for (uint32_t base = 0; base < cnt; base += 32) {
+    const uint2 e = load_edge(base + lane);
     const uint32_t m = min(32u, cnt - base);
-    for (uint32_t j = 0; j < m; j += 4) {
-      uint32_t w[4], wt[4], c0[4], c1[4];
+    for (uint32_t j = 0; j < m; j += 2 * kMsRowsInFlight) {
+      uint32_t ex[kMsRowsInFlight], ey[kMsRowsInFlight];
+      uint4 dw[kMsRowsInFlight];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        w[q] = __shfl_sync(kFull, e.x, (j + q) & 31);
-        wt[q] = __shfl_sync(kFull, e.y, (j + q) & 31);
-        const bool ok = j + q < m;
-        const uint32_t *dw = a.dist + (size_t)w[q] * kMsWidth;
-        c0[q] = ok && lo ? ldcg(dw + lane) : 0u;
-        c1[q] = ok && hi ? ldcg(dw + 32 + lane) : 0u;
+      for (int q = 0; q < kMsRowsInFlight; q++) {
+        const uint32_t idx = j + 2u * q + half;
+        ex[q] = __shfl_sync(kFull, e.x, idx & 31u);
+        ey[q] = ESZ == 8 ? __shfl_sync(kFull, e.y, idx & 31u) : 0u;
+        const uint32_t w = ESZ == 8 ? ex[q] : edge_dst(ex[q], a.wshift);
+        dw[q] = make_uint4(0, 0, 0, 0);
+        if (idx < m && mb)
+          dw[q] = __ldcg(reinterpret_cast<const uint4 *>(a.dist + (size_t)w * kMsWidth) + hl);
       }
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        if (j + q >= m) break;
-        uint32_t *dw = a.dist + (size_t)w[q] * kMsWidth;
-        bool i0 = false, i1 = false;
-        uint32_t best = 0xFFFFFFFFu;
-        const unsigned long long cd0 = (unsigned long long)d0 + wt[q];
-        const unsigned long long cd1 = (unsigned long long)d1 + wt[q];
-        if (lo && cd0 < c0[q] && cd0 < atomicMin(dw + lane, (uint32_t)cd0)) {
-          i0 = true;
-          best = (uint32_t)cd0;
+      for (int q = 0; q < kMsRowsInFlight; q++) {
+        if (j + 2u * q >= m) break;
+        const bool ok = j + 2u * q + half < m;
+        const uint32_t w = ESZ == 8 ? ex[q] : edge_dst(ex[q], a.wshift);
+        const uint32_t wt = ESZ == 8 ? ey[q] : edge_wt(ex[q], a.wshift, a.wbase);
+        uint32_t *row = a.dist + (size_t)w * kMsWidth + 4u * hl;
+        const uint32_t cw[4] = {dw[q].x, dw[q].y, dw[q].z, dw[q].w};
+        uint32_t imp = 0, best = 0xFFFFFFFFu;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const unsigned long long cand = (unsigned long long)du[i] + wt;
+          if (ok && ((mb >> i) & 1u) && cand < cw[i]) {
+            atomicMin(row + i, (uint32_t)cand);
+            imp |= 1u << i;
+            best = min(best, (uint32_t)cand);
+          }
         }
-        if (hi && cd1 < c1[q] && cd1 < atomicMin(dw + 32 + lane, (uint32_t)cd1)) {
-          i1 = true;
-          best = min(best, (uint32_t)cd1);
-        }
-        const unsigned b0 = __ballot_sync(kFull, i0), b1 = __ballot_sync(kFull, i1);
-        if (b0 | b1) {
-          // improving lanes lower the word's pending minimum themselves (one
-          // warp-wide atomic instead of a shuffle reduction)
-          if (i0 || i1) atomicMin(a.wmin + (w[q] >> 5), best);
-          if (lane == 0) {
-            atomicOr(a.front + w[q], (unsigned long long)b0 | ((unsigned long long)b1 << 32));
-            mark_pending<MS_SSSP>(a, w[q]);
+        if (__any_sync(kFull, imp != 0)) {
+          const unsigned b0 = __ballot_sync(kFull, imp & 1u), b1 = __ballot_sync(kFull, imp & 2u);
+          const unsigned b2 = __ballot_sync(kFull, imp & 4u), b3 = __ballot_sync(kFull, imp & 8u);
+          // improving lanes lower the word's pending minimum themselves
+          if (imp) atomicMin(a.wmin + (w >> 5), best);
+          if (hl == 0) {
+            const unsigned sh = 16u * half;
+            const unsigned long long mask =
+                (unsigned long long)((b0 >> sh) & 0xFFFFu) |
+                ((unsigned long long)((b1 >> sh) & 0xFFFFu) << 16) |
+                ((unsigned long long)((b2 >> sh) & 0xFFFFu) << 32) |
+                ((unsigned long long)((b3 >> sh) & 0xFFFFu) << 48);
+            if (mask) {
+              atomicOr(a.front + w, mask);
+              mark_pending<MS_SSSP>(a, w);
+            }
           }
         }
       }
@@ -292,7 +323,7 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long fir
 }
 
 template <int OP, int ESZ, int THREADS>
-__global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
   extern __shared__ uint32_t s_vb[];
   const bool smem_tab = a.nblk <= kSmemBlocks;
   if (smem_tab)
@@ -360,7 +391,7 @@ __global__ void __launch_bounds__(THREADS) ms_kernel(MsArgs a) {
                 r &= r - 1;
               }
 #pragma unroll
-              for (int k = 0; k < 8; k++) d[k] = s[k] >= 0 ? ldcg(dv + s[k]) : 0u;
+              for (int k = 0; k < 8; k++) d[k] = s[k] >= 0 ? ldcg(dv + row_pos((uint32_t)s[k])) : 0u;
 #pragma unroll
               for (int k = 0; k < 8; k++) {
                 if (s[k] < 0) continue;
@@ -522,7 +553,7 @@ __global__ void ms_seed(MsArgs a) {
     atomicOr(a.visit + v, 1ull << s);
     a.lvl[(size_t)v * kMsWidth + s] = 1;
   } else {
-    a.dist[(size_t)v * kMsWidth + s] = 1;
+    a.dist[(size_t)v * kMsWidth + row_pos(s)] = 1;
     atomicMin(a.wmin + (v >> 5), 1u);
   }
 }
@@ -556,7 +587,7 @@ __global__ void ms_extract(MsArgs a, uint32_t *out, unsigned long long *sums) {
           const uint8_t l = a.lvl[v * kMsWidth + s];
           val = l ? l : inf;
         } else {
-          val = a.dist[v * kMsWidth + s];
+          val = a.dist[v * kMsWidth + row_pos(s)];
         }
       }
       tile[dv][s] = val;
