@@ -518,17 +518,17 @@ __global__ void ms_init(MsArgs a, uint32_t nw_alloc) {
   const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   for (uint64_t v = tid; v < a.nv; v += stride) {
     a.front[v] = 0;
-    if (OP == MS_BFS) {
-      a.visit[v] = 0;
-      reinterpret_cast<uint4 *>(a.lvl + v * kMsWidth)[0] = make_uint4(0, 0, 0, 0);
-      reinterpret_cast<uint4 *>(a.lvl + v * kMsWidth)[1] = make_uint4(0, 0, 0, 0);
-      reinterpret_cast<uint4 *>(a.lvl + v * kMsWidth)[2] = make_uint4(0, 0, 0, 0);
-      reinterpret_cast<uint4 *>(a.lvl + v * kMsWidth)[3] = make_uint4(0, 0, 0, 0);
-    } else {
-      uint4 *row = reinterpret_cast<uint4 *>(a.dist + v * kMsWidth);
-      const uint32_t inf = a.nv + 1u;
-      for (int i = 0; i < 16; i++) row[i] = make_uint4(inf, inf, inf, inf);
-    }
+    if (OP == MS_BFS) a.visit[v] = 0;
+  }
+  // per-source rows as one flat array of 16-byte words, consecutive threads
+  // on consecutive words
+  if (OP == MS_BFS) {
+    uint4 *rows = reinterpret_cast<uint4 *>(a.lvl);
+    for (uint64_t i = tid; i < a.nv * (kMsWidth / 16); i += stride) rows[i] = make_uint4(0, 0, 0, 0);
+  } else {
+    uint4 *rows = reinterpret_cast<uint4 *>(a.dist);
+    const uint32_t inf = a.nv + 1u;
+    for (uint64_t i = tid; i < a.nv * (kMsWidth / 4); i += stride) rows[i] = make_uint4(inf, inf, inf, inf);
   }
   for (uint64_t w = tid; w < nw_alloc; w += stride) {
     a.bm[w] = 0;
@@ -566,19 +566,28 @@ __device__ __forceinline__ unsigned long long value_hash(uint32_t v, uint32_t va
   return x ^ (x >> 31);
 }
 
+constexpr uint32_t kExtractThreads = 256;  // ms_extract's block: 32 vertices x 64 sources per tile
+constexpr uint32_t kExtractPer = 32 * kMsWidth / kExtractThreads;
+
 // Per-source values in the single-source encoding: optional k x nv output
 // (rows per source) and a checksum per source (sum of value_hash(v, val)).
+
 template <int OP>
-__global__ void ms_extract(MsArgs a, uint32_t *out, unsigned long long *sums) {
+__global__ void __launch_bounds__(kExtractThreads) ms_extract(MsArgs a, uint32_t *out,
+                                                             unsigned long long *sums) {
   __shared__ unsigned long long s_sum[kMsWidth];
   __shared__ uint32_t tile[32][kMsWidth + 1];
   const uint32_t k = a.sources[0];
   for (uint32_t i = threadIdx.x; i < kMsWidth; i += blockDim.x) s_sum[i] = 0;
+  // a warp always reads sources warp + 8j of a tile (j < kExtractPer), one
+  // vertex per lane: the hashes add up in registers across tiles
+  unsigned long long acc[kExtractPer];
+#pragma unroll
+  for (uint32_t j = 0; j < kExtractPer; j++) acc[j] = 0;
   __syncthreads();
   const uint32_t inf = a.nv + 1u;
-  // blockDim = 256: 32 vertices x 64 sources per tile
   for (uint64_t base = (uint64_t)blockIdx.x * 32; base < a.nv; base += (uint64_t)gridDim.x * 32) {
-    for (uint32_t i = threadIdx.x; i < 32 * kMsWidth; i += blockDim.x) {
+    for (uint32_t i = threadIdx.x; i < 32 * kMsWidth; i += kExtractThreads) {
       const uint32_t dv = i / kMsWidth, s = i % kMsWidth;
       const uint64_t v = base + dv;
       uint32_t val = inf;
@@ -593,20 +602,75 @@ __global__ void ms_extract(MsArgs a, uint32_t *out, unsigned long long *sums) {
       tile[dv][s] = val;
     }
     __syncthreads();
-    for (uint32_t i = threadIdx.x; i < 32 * kMsWidth; i += blockDim.x) {
+#pragma unroll
+    for (uint32_t j = 0; j < kExtractPer; j++) {
+      const uint32_t i = threadIdx.x + j * kExtractThreads;
       const uint32_t s = i / 32, dv = i % 32;
       const uint64_t v = base + dv;
       if (s < k && v < a.nv) {
         const uint32_t val = tile[dv][s];
         if (out) out[(uint64_t)s * a.nv + v] = val;
-        if (sums) atomicAdd(&s_sum[s], value_hash((uint32_t)v, val));
+        acc[j] += value_hash((uint32_t)v, val);
       }
     }
     __syncthreads();
   }
-  if (sums)
-    for (uint32_t i = threadIdx.x; i < k; i += blockDim.x)
-      if (s_sum[i]) atomicAdd(sums + i, s_sum[i]);
+  if (!sums) return;
+#pragma unroll
+  for (uint32_t j = 0; j < kExtractPer; j++) {
+    const unsigned long long t = warp_sum(acc[j]);
+    if (lane_id() == 0 && t) atomicAdd(&s_sum[(threadIdx.x + j * kExtractThreads) / 32], t);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < k; i += blockDim.x)
+    if (s_sum[i]) atomicAdd(sums + i, s_sum[i]);
+}
+
+// Checksums only (no output rows): rows are read as they lie, 16 lanes per
+// row, and each lane keeps the sums of its four sources in registers (SSSP:
+// one 16-byte word = sources l, l+16, l+32, l+48; BFS: one 4-byte word =
+// level bytes of sources 4l..4l+3).
+template <int OP>
+__global__ void __launch_bounds__(kExtractThreads) ms_checksum(MsArgs a, unsigned long long *sums) {
+  __shared__ unsigned long long s_sum[kMsWidth];
+  const uint32_t k = a.sources[0];
+  for (uint32_t i = threadIdx.x; i < kMsWidth; i += blockDim.x) s_sum[i] = 0;
+  __syncthreads();
+  const uint32_t l = threadIdx.x & 15u, inf = a.nv + 1u;
+  uint32_t src[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) src[i] = OP == MS_BFS ? 4u * l + i : l + 16u * i;
+  unsigned long long acc[4] = {0, 0, 0, 0};
+  const uint64_t rows_per = kExtractThreads / 16;
+  for (uint64_t v = (uint64_t)blockIdx.x * rows_per + threadIdx.x / 16; v < a.nv;
+       v += (uint64_t)gridDim.x * rows_per) {
+    uint32_t val[4];
+    if (OP == MS_BFS) {
+      const uint32_t b = __ldcs(reinterpret_cast<const uint32_t *>(a.lvl + v * kMsWidth) + l);
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const uint32_t x = (b >> (8 * i)) & 0xFFu;
+        val[i] = x ? x : inf;
+      }
+    } else {
+      const uint4 d = __ldcs(reinterpret_cast<const uint4 *>(a.dist + v * kMsWidth) + l);
+      val[0] = d.x;
+      val[1] = d.y;
+      val[2] = d.z;
+      val[3] = d.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (src[i] < k) acc[i] += value_hash((uint32_t)v, val[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const unsigned long long t = acc[i] + __shfl_xor_sync(kFull, acc[i], 16);
+    if ((threadIdx.x & 31u) < 16u && t) atomicAdd(&s_sum[src[i]], t);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < k; i += blockDim.x)
+    if (s_sum[i]) atomicAdd(sums + i, s_sum[i]);
 }
 
 // ------------------------------------------------------------------ host --
@@ -762,7 +826,10 @@ static thv_status enqueue_group(thv_graph *g, MsArgs &a, cudaStream_t st, bool w
   THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(grid), dim3(THREADS), args, smem, st));
   THV_CUDA(cudaMemsetAsync(b->d_sums, 0, kMsWidth * 8, st));
   const int xgrid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 31) / 32)));
-  ms_extract<OP><<<xgrid, 256, 0, st>>>(a, want_out ? b->d_out : nullptr, b->d_sums);
+  if (want_out)
+    ms_extract<OP><<<xgrid, kExtractThreads, 0, st>>>(a, b->d_out, b->d_sums);
+  else
+    ms_checksum<OP><<<g->num_sms * 8, kExtractThreads, 0, st>>>(a, b->d_sums);
   THV_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, sizeof(MsCtrl), cudaMemcpyDeviceToHost, st));
   THV_CUDA(cudaMemcpyAsync(b->h_sums, b->d_sums, kMsWidth * 8, cudaMemcpyDeviceToHost, st));
   THV_CUDA(cudaGetLastError());
