@@ -39,9 +39,11 @@ constexpr uint32_t kMsWidth = 64;       // sources per group (mask bits)
 constexpr uint32_t kMaxBfsLevel = 254;  // u8 level bytes hold level + 1
 constexpr uint32_t kMsGrowth = 1;       // SSSP window width factor per advance
 constexpr uint32_t kMsDelta = 256;      // SSSP window width shared by a group
-// SSSP: distance-row loads per lane in flight (two edges each); more spill
-// registers at 64 per thread and run slower
-constexpr int kMsRowsInFlight = 4;
+// SSSP: steps (two edges, one 16-byte row piece per lane each) whose rows
+// are in flight at once, staged through a per-warp shared-memory ring by
+// asynchronous copies (64 KiB per 512-thread block; 12 and 16 measured
+// slower at RMAT-26)
+constexpr uint32_t kMsRing = 8;
 
 // Word of source s in a 64-word SSSP distance row: lane l of a half-warp
 // holds sources l, l+16, l+32, l+48 as one 16-byte word group (4l..4l+3),
@@ -158,84 +160,110 @@ __device__ __forceinline__ void ms_sssp_edge(const MsArgs &a, uint32_t u, uint32
   }
 }
 
+// 16-byte asynchronous global -> shared copy (L2 only); a false `ok`
+// zero-fills the destination without reading.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, bool ok) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+               "r"(ok ? 16 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(addr)
+               : "memory");
+  return v;
+}
+
 // Half-warp-per-edge SSSP relaxation of one work item: the warp loads the
 // item's edges 32 at a time (coalesced); each half-warp takes one edge and
-// reads its whole 256-byte distance row with one 16-byte load per lane
-// (lane l: sources l, l+16, l+32, l+48), so a warp step relaxes two edges
-// for all 64 sources and four steps (eight edges) have their rows in
-// flight together.  Distance updates are fire-and-forget as in
-// ms_sssp_edge; four ballots give each edge's improved-source mask.
+// reads its whole 256-byte distance row, one 16-byte piece per lane (lane
+// l: sources l, l+16, l+32, l+48), so a warp step relaxes two edges for all
+// 64 sources.  The row pieces go through `ring` (this lane's slot of the
+// warp's kMsRing x 512-byte shared ring) by asynchronous copies issued
+// kMsRing steps ahead, so 2 x kMsRing rows are in flight without holding
+// registers.  Each lane reads back only the piece it copied itself.
+// Distance updates are fire-and-forget as in ms_sssp_edge; four ballots
+// give each edge's improved-source mask.
 template <int ESZ>
-__device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t u, uintptr_t eaddr,
-                                             uint32_t cnt, unsigned long long f) {
+__device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t ring, uint32_t u,
+                                             uintptr_t eaddr, uint32_t cnt, unsigned long long f) {
   const unsigned lane = lane_id(), hl = lane & 15u, half = lane >> 4;
   const uint32_t mb = (uint32_t)((f >> hl) & 1ull) | (uint32_t)((f >> (hl + 15u)) & 2ull) |
                       (uint32_t)((f >> (hl + 30u)) & 4ull) | (uint32_t)((f >> (hl + 45u)) & 8ull);
   uint4 du4 = make_uint4(0, 0, 0, 0);
   if (mb) du4 = __ldcg(reinterpret_cast<const uint4 *>(a.dist + (size_t)u * kMsWidth) + hl);
   const uint32_t du[4] = {du4.x, du4.y, du4.z, du4.w};
-  // packed edges stay raw until used (one register per edge in flight)
-  auto load_edge = [&](uint32_t k) {
-    uint2 r = make_uint2(0, 0);
-    if (k < cnt) {
-      if (ESZ == 8) r = ld_nc_u2(eaddr + (uintptr_t)k * 8u);
-      else r.x = ld_nc_u32(eaddr + (uintptr_t)k * 4u);
-    }
-    return r;
-  };
   for (uint32_t base = 0; base < cnt; base += 32) {
-    const uint2 e = load_edge(base + lane);
-    const uint32_t m = min(32u, cnt - base);
-    for (uint32_t j = 0; j < m; j += 2 * kMsRowsInFlight) {
-      uint32_t ex[kMsRowsInFlight], ey[kMsRowsInFlight];
-      uint4 dw[kMsRowsInFlight];
-#pragma unroll
-      for (int q = 0; q < kMsRowsInFlight; q++) {
-        const uint32_t idx = j + 2u * q + half;
-        ex[q] = __shfl_sync(kFull, e.x, idx & 31u);
-        ey[q] = ESZ == 8 ? __shfl_sync(kFull, e.y, idx & 31u) : 0u;
-        const uint32_t w = ESZ == 8 ? ex[q] : edge_dst(ex[q], a.wshift);
-        dw[q] = make_uint4(0, 0, 0, 0);
-        if (idx < m && mb)
-          dw[q] = __ldcg(reinterpret_cast<const uint4 *>(a.dist + (size_t)w * kMsWidth) + hl);
+    // packed edges stay raw until used
+    uint2 e = make_uint2(0, 0);
+    if (base + lane < cnt) {
+      if (ESZ == 8) e = ld_nc_u2(eaddr + (uintptr_t)(base + lane) * 8u);
+      else e.x = ld_nc_u32(eaddr + (uintptr_t)(base + lane) * 4u);
+    }
+    const uint32_t m = min(32u, cnt - base), nsteps = (m + 1) / 2;
+    // step st: edges 2st (lanes 0-15) and 2st+1 (lanes 16-31); one copy
+    // group per step, empty past the end, so group st completes step st
+    auto issue = [&](uint32_t st) {
+      if (st < nsteps) {
+        const uint32_t idx = 2u * st + half;
+        const uint32_t x = __shfl_sync(kFull, e.x, idx & 31u);
+        const uint32_t w = ESZ == 8 ? x : edge_dst(x, a.wshift);
+        const bool ok = idx < m && mb;
+        cp_async16(ring + (st % kMsRing) * 512u,
+                   ok ? (const void *)(a.dist + (size_t)w * kMsWidth + 4u * hl) : (const void *)a.dist,
+                   ok);
       }
+      cp_async_commit();
+    };
 #pragma unroll
-      for (int q = 0; q < kMsRowsInFlight; q++) {
-        if (j + 2u * q >= m) break;
-        const bool ok = j + 2u * q + half < m;
-        const uint32_t w = ESZ == 8 ? ex[q] : edge_dst(ex[q], a.wshift);
-        const uint32_t wt = ESZ == 8 ? ey[q] : edge_wt(ex[q], a.wshift, a.wbase);
-        uint32_t *row = a.dist + (size_t)w * kMsWidth + 4u * hl;
-        const uint32_t cw[4] = {dw[q].x, dw[q].y, dw[q].z, dw[q].w};
-        uint32_t imp = 0, best = 0xFFFFFFFFu;
+    for (uint32_t st = 0; st < kMsRing; st++) issue(st);
+    for (uint32_t st = 0; st < nsteps; st++) {
+      cp_async_wait<kMsRing - 1>();
+      const uint4 dw = lds128(ring + (st % kMsRing) * 512u);
+      const uint32_t idx = 2u * st + half;
+      const uint32_t x = __shfl_sync(kFull, e.x, idx & 31u);
+      const uint32_t y = ESZ == 8 ? __shfl_sync(kFull, e.y, idx & 31u) : 0u;
+      const bool ok = idx < m;
+      const uint32_t w = ESZ == 8 ? x : edge_dst(x, a.wshift);
+      const uint32_t wt = ESZ == 8 ? y : edge_wt(x, a.wshift, a.wbase);
+      uint32_t *row = a.dist + (size_t)w * kMsWidth + 4u * hl;
+      const uint32_t cw[4] = {dw.x, dw.y, dw.z, dw.w};
+      uint32_t imp = 0, best = 0xFFFFFFFFu;
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-          const unsigned long long cand = (unsigned long long)du[i] + wt;
-          if (ok && ((mb >> i) & 1u) && cand < cw[i]) {
-            atomicMin(row + i, (uint32_t)cand);
-            imp |= 1u << i;
-            best = min(best, (uint32_t)cand);
-          }
-        }
-        if (__any_sync(kFull, imp != 0)) {
-          const unsigned b0 = __ballot_sync(kFull, imp & 1u), b1 = __ballot_sync(kFull, imp & 2u);
-          const unsigned b2 = __ballot_sync(kFull, imp & 4u), b3 = __ballot_sync(kFull, imp & 8u);
-          // improving lanes lower the word's pending minimum themselves
-          if (imp) atomicMin(a.wmin + (w >> 5), best);
-          if (hl == 0) {
-            const unsigned sh = 16u * half;
-            const unsigned long long mask =
-                (unsigned long long)((b0 >> sh) & 0xFFFFu) |
-                ((unsigned long long)((b1 >> sh) & 0xFFFFu) << 16) |
-                ((unsigned long long)((b2 >> sh) & 0xFFFFu) << 32) |
-                ((unsigned long long)((b3 >> sh) & 0xFFFFu) << 48);
-            if (mask) {
-              atomicOr(a.front + w, mask);
-              mark_pending<MS_SSSP>(a, w);
-            }
-          }
+      for (int i = 0; i < 4; i++) {
+        const unsigned long long cand = (unsigned long long)du[i] + wt;
+        if (ok && ((mb >> i) & 1u) && cand < cw[i]) {
+          atomicMin(row + i, (uint32_t)cand);
+          imp |= 1u << i;
+          best = min(best, (uint32_t)cand);
         }
       }
+      if (__any_sync(kFull, imp != 0)) {
+        const unsigned b0 = __ballot_sync(kFull, imp & 1u), b1 = __ballot_sync(kFull, imp & 2u);
+        const unsigned b2 = __ballot_sync(kFull, imp & 4u), b3 = __ballot_sync(kFull, imp & 8u);
+        // improving lanes lower the word's pending minimum themselves
+        if (imp) atomicMin(a.wmin + (w >> 5), best);
+        if (hl == 0) {
+          const unsigned sh = 16u * half;
+          const unsigned long long mask =
+              (unsigned long long)((b0 >> sh) & 0xFFFFu) |
+              ((unsigned long long)((b1 >> sh) & 0xFFFFu) << 16) |
+              ((unsigned long long)((b2 >> sh) & 0xFFFFu) << 32) |
+              ((unsigned long long)((b3 >> sh) & 0xFFFFu) << 48);
+          if (mask) {
+            atomicOr(a.front + w, mask);
+            mark_pending<MS_SSSP>(a, w);
+          }
+        }
+      }
+      issue(st + kMsRing);
     }
   }
 }
@@ -251,10 +279,10 @@ __device__ __forceinline__ void ms_edge(const MsArgs &a, uint32_t u, uint32_t w,
 }
 
 template <int OP, int ESZ>
-__device__ __forceinline__ void ms_chunk(const MsArgs &a, const WorkItem &it,
+__device__ __forceinline__ void ms_chunk(const MsArgs &a, uint32_t ring, const WorkItem &it,
                                          unsigned long long f, uint32_t lvl1) {
   if (OP == MS_SSSP && __popcll(f) > kSparseMask) {
-    ms_sssp_item<ESZ>(a, it.v, it.eaddr, it.cnt, f);
+    ms_sssp_item<ESZ>(a, ring, it.v, it.eaddr, it.cnt, f);
     return;
   }
   constexpr int PER = 16 / ESZ;
@@ -275,7 +303,7 @@ __device__ __forceinline__ void ms_chunk(const MsArgs &a, const WorkItem &it,
 }
 
 template <int OP, int ESZ>
-__device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long first,
+__device__ __forceinline__ void ms_group(const MsArgs &a, uint32_t ring, unsigned long long first,
                                          unsigned long long n_small, uint32_t lvl1) {
   const unsigned lane = lane_id();
   const unsigned long long idx = first + lane;
@@ -291,7 +319,7 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long fir
     while (dense) {
       const int i = __ffs(dense) - 1;
       dense &= dense - 1;
-      ms_sssp_item<ESZ>(a, __shfl_sync(kFull, it.v, i), (uintptr_t)shfl64(it.eaddr, i),
+      ms_sssp_item<ESZ>(a, ring, __shfl_sync(kFull, it.v, i), (uintptr_t)shfl64(it.eaddr, i),
                    __shfl_sync(kFull, it.cnt, i), shfl64(f, i));
     }
     if (__popcll(f) > kSparseMask) {
@@ -324,7 +352,12 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, unsigned long long fir
 
 template <int OP, int ESZ, int THREADS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
-  extern __shared__ uint32_t s_vb[];
+  // dynamic shared memory: SSSP's per-warp rings, then the block table
+  extern __shared__ uint4 s_dyn[];
+  constexpr uint32_t ring_words = OP == MS_SSSP ? THREADS / 32 * kMsRing * 32 : 0;
+  uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_dyn + ring_words);
+  const uint32_t ring = (uint32_t)__cvta_generic_to_shared(s_dyn) +
+                        ((threadIdx.x >> 5) * kMsRing * 32u + (threadIdx.x & 31u)) * 16u;
   const bool smem_tab = a.nblk <= kSmemBlocks;
   if (smem_tab)
     for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x) s_vb[i] = a.blk_vb[i];
@@ -500,8 +533,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
     const uint32_t lvl1 = level + 1;
     const unsigned long long ntask = nb + (ns + 31) / 32;
     for (unsigned long long t = gwarp; t < ntask;) {
-      if (t < nb) ms_chunk<OP, ESZ>(a, a.qb[t], a.qbm[t], lvl1);
-      else ms_group<OP, ESZ>(a, (t - nb) * 32ull, ns, lvl1);
+      if (t < nb) ms_chunk<OP, ESZ>(a, ring, a.qb[t], a.qbm[t], lvl1);
+      else ms_group<OP, ESZ>(a, ring, (t - nb) * 32ull, ns, lvl1);
       unsigned long long nt = 0;
       if (lane == 0) nt = nwarps + atomicAdd(&c->wc[slot], 1ull);
       t = shfl64(nt, 0);
@@ -813,7 +846,9 @@ template <int OP, int ESZ, int THREADS>
 static thv_status enqueue_group(thv_graph *g, MsArgs &a, cudaStream_t st, bool want_out) {
   BatchState *b = g->bs;
   auto kern = ms_kernel<OP, ESZ, THREADS>;
-  const size_t smem = g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0;
+  const size_t ring = OP == MS_SSSP ? (size_t)THREADS / 32 * kMsRing * 512 : 0;
+  const size_t smem = ring + (g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0);
+  THV_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int bpsm = 0;
   THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, THREADS, smem));
   if (bpsm < 1) return fail(THV_ECUDA, "batch kernel cannot be resident");
