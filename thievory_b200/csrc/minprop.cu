@@ -171,6 +171,10 @@ __device__ __forceinline__ void relax_n(const MinArgs &a, const uint32_t (&w)[N]
   }
 }
 
+__device__ __forceinline__ uint32_t sat32(unsigned long long x) {
+  return x > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)x;
+}
+
 template <int OP>
 __device__ __forceinline__ unsigned long long candidate(uint32_t vval, uint32_t wt) {
   return OP == OP_BFS    ? (unsigned long long)vval + 1ull
@@ -655,40 +659,65 @@ struct QEnv {
   unsigned cs_next;
   uint32_t thr;
   uint32_t tag;  // tag of the output queue: phase + 1
+  uint2 *stage;  // this warp's shared list of vertices to queue: (w, value)
 };
 
+// Queue-mode relaxation: up to this many edges per lane in one call.
+constexpr int kQRelaxMax = 8;
+
 // Relax N edges per lane; near improvements are queued, far ones parked.
+// Each dependent step (value probe, atomicMin, tag probe, tag atomicMax) is
+// issued for all N edges before any result is used, so a lane has N
+// requests in flight per step instead of one.  The vertices to queue are
+// staged in the warp's shared list and appended 32 at a time: one
+// warp-aggregated reservation per 32 queued vertices instead of one per
+// edge slot.  cand is the saturated u32 candidate (0xFFFFFFFF never wins).
 template <int OP, int ESZ, int N>
 __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const uint32_t (&w)[N],
-                                          const unsigned long long (&cand)[N], const bool (&ok)[N],
+                                          const uint32_t (&cand)[N], const bool (&ok)[N],
                                           QStats &qst) {
-  uint32_t cur[N];
+  static_assert(N <= kQRelaxMax, "staging list holds kQRelaxMax entries per lane");
+  uint32_t r[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) r[j] = ok[j] ? ldcg(a.val + w[j]) : 0u;
+#pragma unroll
+  for (int j = 0; j < N; j++) r[j] = ok[j] && cand[j] < r[j] ? atomicMin(a.val + w[j], cand[j]) : 0u;
   bool push[N];
 #pragma unroll
-  for (int j = 0; j < N; j++) cur[j] = ok[j] ? ldcg(a.val + w[j]) : 0u;
-#pragma unroll
   for (int j = 0; j < N; j++) {
-    push[j] = false;
-    if (ok[j] && cand[j] < cur[j]) {
-      const uint32_t old = atomicMin(a.val + w[j], (uint32_t)cand[j]);
-      if (cand[j] < old) {
-        if (OP == OP_BFS) {
-          push[j] = true;
-        } else if (cand[j] < e.thr) {
-          push[j] = ldcg(a.qtag + w[j]) != e.tag && atomicMax(a.qtag + w[j], e.tag) < e.tag;
-        } else {
-          atomicMin(a.wmin + (w[j] >> 5), (uint32_t)cand[j]);
-          const uint32_t m = 1u << (w[j] & 31u);
-          uint32_t *bp = a.bm + (w[j] >> 5);
-          if (!(ldcg(bp) & m)) atomicOr(bp, m);
-        }
-      }
+    const bool imp = cand[j] < r[j];  // 0 when not attempted
+    push[j] = imp && (OP == OP_BFS || cand[j] < e.thr);
+    if (OP != OP_BFS && imp && !push[j]) {
+      atomicMin(a.wmin + (w[j] >> 5), cand[j]);
+      const uint32_t m = 1u << (w[j] & 31u);
+      uint32_t *bp = a.bm + (w[j] >> 5);
+      if (!(ldcg(bp) & m)) atomicOr(bp, m);
     }
   }
+  if (OP != OP_BFS) {
 #pragma unroll
-  for (int j = 0; j < N; j++)
-    q_append<ESZ>(a, e.vb, e.bbase, e.qs_next, e.qb_next, e.cs_next, push[j], w[j],
-                  (uint32_t)cand[j], qst);
+    for (int j = 0; j < N; j++) r[j] = push[j] ? ldcg(a.qtag + w[j]) : e.tag;
+#pragma unroll
+    for (int j = 0; j < N; j++) r[j] = r[j] != e.tag ? atomicMax(a.qtag + w[j], e.tag) : e.tag;
+#pragma unroll
+    for (int j = 0; j < N; j++) push[j] = push[j] && r[j] < e.tag;
+  }
+  const unsigned lane = lane_id();
+  unsigned n = 0;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    const unsigned b = __ballot_sync(kFull, push[j]);
+    if (push[j]) e.stage[n + __popc(b & lanemask_lt())] = make_uint2(w[j], cand[j]);
+    n += __popc(b);
+  }
+  if (!n) return;
+  __syncwarp();
+  for (unsigned k = 0; k < n; k += 32) {
+    const bool f = k + lane < n;
+    const uint2 x = f ? e.stage[k + lane] : make_uint2(0, 0);
+    q_append<ESZ>(a, e.vb, e.bbase, e.qs_next, e.qb_next, e.cs_next, f, x.x, x.y, qst);
+  }
+  __syncwarp();
 }
 
 // Dequeue: BFS values are final when queued.  SSSP/CC clear the vertex's
@@ -728,8 +757,7 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
 #pragma unroll
     for (int h = 0; h < 2; h++)
       q[h] = p + 512u * h < end ? ld_nc_v4(p + 512u * h) : make_uint4(0, 0, 0, 0);
-    uint32_t w[2 * PER];
-    unsigned long long cand[2 * PER];
+    uint32_t w[2 * PER], cand[2 * PER];
     bool ok[2 * PER];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -740,7 +768,7 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
         const int k = h * PER + j;
         ok[k] = ea >= start && ea < end;
         w[k] = ESZ == 4 ? edge_dst(f[j], a.wshift) : f[2 * j];
-        cand[k] = candidate<OP>(vval, ESZ == 4 ? edge_wt(f[j], a.wshift, a.wbase) : f[2 * j + 1]);
+        cand[k] = sat32(candidate<OP>(vval, ESZ == 4 ? edge_wt(f[j], a.wshift, a.wbase) : f[2 * j + 1]));
       }
     }
     q_relax_n<OP, ESZ, 2 * PER>(a, e, w, cand, ok, qst);
@@ -767,8 +795,7 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
   const unsigned total = __shfl_sync(kFull, incl, 31);
   // 64 edges per step, two per lane in flight
   for (unsigned k = 0; k < total; k += 64) {
-    uint32_t w[2] = {0, 0};
-    unsigned long long cand[2];
+    uint32_t w[2] = {0, 0}, cand[2];
     bool ok[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -791,7 +818,7 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
           wt = ed.y;
         }
       }
-      cand[h] = candidate<OP>(ov, wt);
+      cand[h] = sat32(candidate<OP>(ov, wt));
     }
     q_relax_n<OP, ESZ, 2>(a, e, w, cand, ok, qst);
   }
@@ -801,6 +828,7 @@ template <int OP, int ESZ>
 // Two blocks per SM: 64 registers, no spills (3 blocks spill and measured slower).
 __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
   extern __shared__ unsigned long long s_tab[];
+  __shared__ uint2 s_stage[kMinThreads / 32][32 * kQRelaxMax];
   const bool smem_tab = a.nblk <= kSmemBlocks;
   unsigned long long *s_base = s_tab;
   uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_tab + a.nblk);
@@ -812,6 +840,7 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
   QEnv env;
   env.vb = smem_tab ? s_vb : a.blk_vb;
   env.bbase = smem_tab ? s_base : (const unsigned long long *)a.blk_base;
+  env.stage = s_stage[threadIdx.x >> 5];
   MinCtrl *c = a.ctrl;
   const unsigned lane = lane_id();
   const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1271,6 +1300,7 @@ static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
   auto kern = scan_mode ? minprop_kernel<OP, ESZ> : minq_kernel<OP, ESZ>;
   const size_t nb = g->plan.blocks.size();
   const size_t smem = nb <= kSmemBlocks ? nb * 8 + (nb + 1) * 4 : 0;
+  THV_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int bpsm = 0;
   THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern,
                                                          kMinThreads, smem));
