@@ -664,6 +664,23 @@ struct QEnv {
 
 // Queue-mode relaxation: up to this many edges per lane in one call.
 constexpr int kQRelaxMax = 8;
+// Queue-mode scan: pending vertices probed per lane per step.
+constexpr int kScanPer = 4;
+
+// Position of the n-th (from 0) set bit of x; n < popc(x).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t n) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t s = 16; s > 0; s >>= 1) {
+    const uint32_t lo = __popc(x & ((1u << s) - 1u));
+    if (n >= lo) {
+      n -= lo;
+      x >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
 
 // Relax N edges per lane; near improvements are queued, far ones parked.
 // Each dependent step (value probe, atomicMin, tag probe, tag atomicMax) is
@@ -829,6 +846,7 @@ template <int OP, int ESZ>
 __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
   extern __shared__ unsigned long long s_tab[];
   __shared__ uint2 s_stage[kMinThreads / 32][32 * kQRelaxMax];
+  __shared__ uint32_t s_word[kMinThreads / 32][64];  // scan: taken bits, least kept value per word
   const bool smem_tab = a.nblk <= kSmemBlocks;
   unsigned long long *s_base = s_tab;
   uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_tab + a.nblk);
@@ -881,40 +899,76 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
     env.tag = ph + 1;
     if (scan) {
       // ------------------------------------------------------------- scan
+      // A warp owns 32 bitmap words (lane = word).  The pending vertices of
+      // the words inside the window are numbered across the warp and probed
+      // kScanPer x 32 at a time (independent loads, however sparse the
+      // words); per-word results gather in shared memory (taken bits, least
+      // kept value) and the words are rewritten once at the end.
       unsigned long long my_keep = 0;
       uint32_t my_min = 0xFFFFFFFFu;
+      uint32_t *s_tk = s_word[threadIdx.x >> 5], *s_km = s_tk + 32;
       for (unsigned g = gwarp; g < a.ngroups; g += nwarps) {
         const unsigned wbase = g * 32u;
         const uint32_t word = ldcg(a.bm + wbase + lane);
-        unsigned nz = __ballot_sync(kFull, word != 0);
+        bool act_word = word != 0;
         if (OP != OP_BFS) {
           const uint32_t wm = word ? ldcg(a.wmin + wbase + lane) : 0xFFFFFFFFu;
           if (word != 0 && wm >= thr) {
             my_keep += __popc(word);
             my_min = min(my_min, wm);
+            act_word = false;
           }
-          nz = __ballot_sync(kFull, word != 0 && wm < thr);
         }
-        while (nz) {
-          const int j = __ffs(nz) - 1;
-          nz &= nz - 1;
-          const uint32_t wd = __shfl_sync(kFull, word, j);
-          const uint32_t v = (wbase + j) * 32u + lane;
-          const bool act = (wd >> lane) & 1u;
-          const uint32_t vval = act ? ldcg(a.val + v) : 0u;
-          const bool take = act && (OP == OP_BFS || vval < thr);
-          const unsigned tm = __ballot_sync(kFull, take);
+        const unsigned cnt = act_word ? (unsigned)__popc(word) : 0u;
+        const unsigned incl = warp_incl_scan<unsigned>(cnt);
+        const unsigned excl = incl - cnt, total = __shfl_sync(kFull, incl, 31);
+        if (total == 0) continue;
+        s_tk[lane] = 0;
+        s_km[lane] = 0xFFFFFFFFu;
+        __syncwarp();
+        for (unsigned k = 0; k < total; k += 32u * kScanPer) {
+          uint32_t v[kScanPer], vv[kScanPer];
+          int own[kScanPer];
+#pragma unroll
+          for (int i = 0; i < kScanPer; i++) {
+            const unsigned t = k + 32u * i + lane;
+            own[i] = warp_owner(excl, t);
+            const uint32_t ow = __shfl_sync(kFull, word, own[i]);
+            const unsigned oex = __shfl_sync(kFull, excl, own[i]);
+            v[i] = t < total ? (wbase + own[i]) * 32u + nth_set_bit(ow, t - oex) : 0xFFFFFFFFu;
+          }
+#pragma unroll
+          for (int i = 0; i < kScanPer; i++) vv[i] = v[i] != 0xFFFFFFFFu ? ldcg(a.val + v[i]) : 0u;
+          unsigned n = 0;
+#pragma unroll
+          for (int i = 0; i < kScanPer; i++) {
+            const bool in = v[i] != 0xFFFFFFFFu;
+            const bool take = in && (OP == OP_BFS || vv[i] < thr);
+            if (take) atomicOr(&s_tk[own[i]], 1u << (v[i] & 31u));
+            else if (OP != OP_BFS && in) atomicMin(&s_km[own[i]], vv[i]);
+            const unsigned b = __ballot_sync(kFull, take);
+            if (take) env.stage[n + __popc(b & lanemask_lt())] = make_uint2(v[i], vv[i]);
+            n += __popc(b);
+          }
+          __syncwarp();
+          for (unsigned kk = 0; kk < n; kk += 32) {
+            const bool f = kk + lane < n;
+            const uint2 x = f ? env.stage[kk + lane] : make_uint2(0, 0);
+            q_append<ESZ>(a, env.vb, env.bbase, qs_out, qb_out, cur, f, x.x, x.y, qst);
+          }
+          __syncwarp();
+        }
+        if (act_word) {
+          const uint32_t tk = s_tk[lane];
           if (OP != OP_BFS) {
-            const uint32_t kmin = warp_min(act && !take ? vval : 0xFFFFFFFFu);
-            my_min = min(my_min, kmin);
-            if (lane == 0) {
-              my_keep += __popc(wd & ~tm);
-              a.wmin[wbase + j] = kmin;
-            }
+            const uint32_t km = s_km[lane];
+            a.wmin[wbase + lane] = km;
+            my_keep += __popc(word & ~tk);
+            my_min = min(my_min, km);
           }
-          if (lane == 0 && tm) a.bm[wbase + j] = wd & ~tm;
-          q_append<ESZ>(a, env.vb, env.bbase, qs_out, qb_out, cur, take, v, vval, qst);
+          if (tk) a.bm[wbase + lane] = word & ~tk;
         }
+        __syncwarp();
       }
       if (OP != OP_BFS) {
         my_keep = warp_sum(my_keep);
