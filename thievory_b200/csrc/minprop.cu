@@ -666,6 +666,9 @@ struct QEnv {
 constexpr int kQRelaxMax = 8;
 // Queue-mode scan: pending vertices probed per lane per step.
 constexpr int kScanPer = 4;
+// Queue-mode small-vertex groups: edges per lane per step (2 and 4
+// measured slower at RMAT-24).
+constexpr int kGroupPer = 8;
 
 // Position of the n-th (from 0) set bit of x; n < popc(x).
 __device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t n) {
@@ -810,12 +813,13 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
   const unsigned incl = warp_incl_scan<unsigned>(cnt);
   const unsigned excl = incl - cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
-  // 64 edges per step, two per lane in flight
-  for (unsigned k = 0; k < total; k += 64) {
-    uint32_t w[2] = {0, 0}, cand[2];
-    bool ok[2];
+  // kGroupPer x 32 edges per step, kGroupPer per lane in flight
+  for (unsigned k = 0; k < total; k += 32u * kGroupPer) {
+    uint32_t w[kGroupPer], cand[kGroupPer];
+    bool ok[kGroupPer];
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
+    for (int h = 0; h < kGroupPer; h++) {
+      w[h] = 0;
       const unsigned t = k + 32u * h + lane;
       const int o = warp_owner(excl, t);
       const unsigned long long ea = shfl64(eaddr, o);
@@ -837,7 +841,7 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
       }
       cand[h] = sat32(candidate<OP>(ov, wt));
     }
-    q_relax_n<OP, ESZ, 2>(a, e, w, cand, ok, qst);
+    q_relax_n<OP, ESZ, kGroupPer>(a, e, w, cand, ok, qst);
   }
 }
 
