@@ -79,6 +79,21 @@ def test_batched_checksums_only(T, O, g14w):
             assert int(sums[i]) == T.values_checksum(vals)
 
 
+@pytest.mark.parametrize("algo", ["bfs", "sssp"])
+def test_checksum_only_groups_match_single_runs(T, O, g14w, algo):
+    """Without output rows the checksums come from a streaming pass over the
+    per-source rows; a full group and a partial one (37 of 64 sources) must
+    give the single runs' checksums."""
+    src = sources(O, g14w, 64 + 37)
+    ref = O.sssp if algo == "sssp" else O.bfs
+    with T.Graph.from_arrays(g14w.off, g14w.wcsr_edges(), "wcsr") as g:
+        g.plan(int(0.4 * g.ne * 8), block_bytes=BLOCK)
+        out, sums, _ = g.batch_run(algo, src, want_values=False, timeout_ms=20000)
+        assert out is None
+        for i in sorted(set(range(0, len(src), 9)) | {1, 63, 64, len(src) - 1}):
+            assert int(sums[i]) == T.values_checksum(ref(g14w, int(src[i]))), (algo, i)
+
+
 def test_batched_tuning_is_result_neutral(T, O, g14):
     src = sources(O, g14, 64)
     with T.Graph.from_arrays(g14.off, g14.adj, "csr") as g:

@@ -131,6 +131,32 @@ __device__ __forceinline__ void ms_bfs_edge(const MsArgs &a, uint32_t w,
   }
 }
 
+// BFS edges w[j] for the source masks f[j] (0: no edge), N per lane: the
+// visit probes, then the claiming atomicOr's, are issued for all N edges
+// before any result is used, so a lane has N requests in flight per step.
+template <int N>
+__device__ __forceinline__ void ms_bfs_edges(const MsArgs &a, const uint32_t (&w)[N],
+                                             const unsigned long long (&f)[N], uint32_t lvl1) {
+  unsigned long long m[N];
+#pragma unroll
+  for (int j = 0; j < N; j++) m[j] = f[j] ? f[j] & ~ldcg(a.visit + w[j]) : 0ull;
+#pragma unroll
+  for (int j = 0; j < N; j++) m[j] = m[j] ? m[j] & ~atomicOr(a.visit + w[j], m[j]) : 0ull;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    unsigned long long nb = m[j];
+    if (!nb) continue;
+    atomicOr(a.front + w[j], nb);
+    mark_pending<MS_BFS>(a, w[j]);
+    uint8_t *row = a.lvl + (size_t)w[j] * kMsWidth;
+    while (nb) {
+      const int s = __ffsll((long long)nb) - 1;
+      nb &= nb - 1;
+      row[s] = (uint8_t)lvl1;
+    }
+  }
+}
+
 // SSSP edge u->w of weight wt for the sources in f.  The distance update
 // is a fire-and-forget atomicMin: when cand is below the value read, (w, s)
 // is marked pending whether this lane or a concurrent one ends up lowering
@@ -270,6 +296,9 @@ __device__ __forceinline__ void ms_sssp_item(const MsArgs &a, uint32_t ring, uin
 
 // masks with at most this many sources relax lane-per-edge instead
 constexpr int kSparseMask = 4;
+// BFS groups of small vertices: edges per lane per step (8 spills at 64
+// registers)
+constexpr int kMsGroupPer = 4;
 
 template <int OP, int ESZ>
 __device__ __forceinline__ void ms_edge(const MsArgs &a, uint32_t u, uint32_t w,
@@ -289,6 +318,27 @@ __device__ __forceinline__ void ms_chunk(const MsArgs &a, uint32_t ring, const W
   const unsigned lane = lane_id();
   const uintptr_t start = it.eaddr;
   const uintptr_t end = start + (uintptr_t)it.cnt * ESZ;
+  if (OP == MS_BFS) {
+    // two 16-byte loads per lane per step, all their edges probed together
+    for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end; p += 1024u) {
+      uint32_t w[2 * PER];
+      unsigned long long fm[2 * PER];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const uintptr_t ph = p + 512u * h;
+        const uint4 q = ph < end ? ld_nc_v4(ph) : make_uint4(0, 0, 0, 0);
+        const uint32_t e[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int j = 0; j < PER; j++) {
+          const uintptr_t ea = ph + (uintptr_t)ESZ * j;
+          w[h * PER + j] = ESZ == 4 ? edge_dst(e[j], a.wshift) : e[2 * j];
+          fm[h * PER + j] = ea >= start && ea < end ? f : 0ull;
+        }
+      }
+      ms_bfs_edges<2 * PER>(a, w, fm, lvl1);
+    }
+    return;
+  }
   for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end; p += 512u) {
     const uint4 q = ld_nc_v4(p);
     const uint32_t e[4] = {q.x, q.y, q.z, q.w};
@@ -330,6 +380,30 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, uint32_t ring, unsigne
   const unsigned incl = warp_incl_scan<unsigned>(it.cnt);
   const unsigned excl = incl - it.cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
+  if (OP == MS_BFS) {
+    // kMsGroupPer edges per lane per step, probed together
+    for (unsigned k = 0; k < total; k += 32u * kMsGroupPer) {
+      uint32_t w[kMsGroupPer];
+      unsigned long long fm[kMsGroupPer];
+#pragma unroll
+      for (int h = 0; h < kMsGroupPer; h++) {
+        const unsigned t = k + 32u * h + lane;
+        const int o = warp_owner(excl, t);
+        const unsigned long long ea = shfl64(it.eaddr, o);
+        const unsigned oex = __shfl_sync(kFull, excl, o);
+        const unsigned long long of = shfl64(f, o);
+        w[h] = 0;
+        fm[h] = 0;
+        if (t < total) {
+          const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
+          w[h] = ESZ == 4 ? edge_dst(ld_nc_u32(addr), a.wshift) : ld_nc_u2(addr).x;
+          fm[h] = of;
+        }
+      }
+      ms_bfs_edges<kMsGroupPer>(a, w, fm, lvl1);
+    }
+    return;
+  }
   for (unsigned k = 0; k < total; k += 32) {
     const unsigned t = k + lane;
     const int o = warp_owner(excl, t);
