@@ -15,7 +15,7 @@ pytestmark = pytest.mark.gpu
 
 BUDGETS = [0.0, 0.4, 1.0]
 BLOCK = 64 << 10  # 64 KiB blocks: many blocks even on small graphs
-PR_RTOL = 1e-6    # north-star PageRank tolerance (max per-vertex relative)
+PR_RTOL = 1e-6    # PageRank: max per-vertex relative error against the FP64 oracle
 
 
 @pytest.fixture(scope="module")
