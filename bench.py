@@ -45,7 +45,7 @@ FALLBACK_HBM_GBS = 6650.0
 # made on a smaller graph are scaled to the bench size by edge count (the
 # traffic of these kernels grows with the edges traversed).
 NCU_TRAFFIC = {
-    "sssp": dict(scale=22, ne=65241959, dram=596816896 + 86474240, sysmem=3297059 * 32),
+    "sssp": dict(scale=22, ne=65241959, dram=597834496 + 83409920, sysmem=3283365 * 32),
     "cc": dict(scale=22, ne=128306542, dram=392704512 + 69563648, sysmem=11788847 * 32),
     "bfs": dict(scale=20, ne=16084564, dram=41359616 + 613888, sysmem=0),
     "pr_pull": dict(scale=22, ne=65241959, dram=135399168 + 20317184, sysmem=6104134 * 32, per="iteration"),
