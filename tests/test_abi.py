@@ -100,3 +100,17 @@ def test_cli_missing_file(root, tmp_path):
 def test_cli_bad_edge_size(root):
     r = run_main(root, "--input", "x.csr", "--edgeSize", "3")
     assert r.returncode == 1
+
+
+def test_convert_input_errors_before_any_device_work(T, tmp_path):
+    """thv_convert checks its arguments and parses the whole text file on
+    the host before it touches a GPU: these errors come back on any host."""
+    with pytest.raises(T.ThvError) as e:
+        T.convert(str(tmp_path / "missing.txt"), str(tmp_path / "o.csr"))
+    assert e.value.status == T.THV_EIO
+    txt = tmp_path / "g.txt"
+    txt.write_text("0 1\n1 4294967295\n")
+    with pytest.raises(T.ThvError) as e:
+        T.convert(str(txt), str(tmp_path / "o.csr"), skip=0)
+    assert e.value.status == T.THV_EUNSUPPORTED
+    assert not (tmp_path / "o.csr").exists()
