@@ -334,7 +334,7 @@ class Graph:
             sssp_growth: int = 0, top_down_only: bool = False, label_propagation: bool = False):
         """Run algo; returns (values or None, stats dict).  compaction:
         "" (per-algorithm default), "scan" or "queue"; sssp_growth: SSSP
-        window growth per advance (0 = default 8, 1 = fixed windows)."""
+        window growth per advance (0 = default 16, 1 = fixed windows)."""
         lib = load_library()
         flags = ((1 if checksum else 0) | (2 if compaction == "scan" else 0)
                  | (4 if compaction == "queue" else 0) | (8 if top_down_only else 0)
