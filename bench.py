@@ -412,10 +412,11 @@ def run_batched(args, dist):
         dl = args.sssp_delta if algo == "sssp" else 0
         g.batch_run(algo, src[:64], want_values=False, sssp_delta=dl, tune=True)  # tunes, warms up
         _, sums, bst = g.batch_run(algo, src, want_values=False, sssp_delta=dl, tune=True)
-        plain_ms = []
+        plain_ms, plain_bytes = [], []
         for s_ in src[: args.plain_sample]:
             vals, st = g.run(algo, source=int(s_))
             plain_ms.append(st["device_ms"])
+            plain_bytes.append(st["hbm_edge_bytes"] + st["link_edge_bytes"])
             i = int(np.nonzero(src == s_)[0][0])
             assert T.values_checksum(vals) == int(sums[i]), f"{algo} source {s_} differs"
         qps_b = dist.n * len(src) / (dist.max(bst["device_ms"]) / 1e3)
@@ -425,6 +426,10 @@ def run_batched(args, dist):
                      "batched_ms_total": bst["device_ms"], "plain_ms_mean": statistics.mean(plain_ms),
                      "queries": len(src), "plain_sample": args.plain_sample,
                      "batched_link_bytes": bst["link_edge_bytes"], "batched_iterations": bst["iterations"],
+                     # edge bytes read: all groups together vs the plain form
+                     # (sampled mean per query x queries)
+                     "batched_edge_bytes": bst["hbm_edge_bytes"] + bst["link_edge_bytes"],
+                     "plain_form_edge_bytes": statistics.mean(plain_bytes) * len(src),
                      "checked": f"{args.plain_sample} sources: single-run checksum == batched checksum"}
         g.close()
     return scale, out
