@@ -1,0 +1,55 @@
+"""The roofline denominators bench.py reports: algorithmic bytes of a
+work-optimal run, split into HBM and host-link bytes, on hand-counted toy
+graphs (no GPU needed)."""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+ROOT = os.path.join(os.path.dirname(__file__), "..")
+
+
+@pytest.fixture(scope="module")
+def bench():
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+# 4 vertices, degrees 2, 1, 0, 2; blocks {0, 1} (resident) and {2, 3} (host)
+OFF = np.array([0, 2, 3, 3, 5], np.uint64)
+VB = np.array([0, 2, 4], np.uint32)
+RES = np.array([True, False])
+
+
+def test_traversal_bytes_split_by_residency(bench):
+    vals = np.array([1, 2, 5, 3], np.uint32)  # vertex 2 unreached (n + 1)
+    hbm, link, edges = bench.algorithmic_bytes(OFF, vals, 4, VB, RES, 4, "sssp")
+    # reached: 0, 1 (resident, 3 edges) and 3 (host, 2 edges)
+    assert link == 2 * 4
+    assert hbm == 3 * 4 + 5 * 4 + 3 * (16 + 4)
+    assert edges == 5
+
+
+def test_small_list_cache_moves_short_host_lists_to_hbm(bench):
+    vals = np.array([1, 2, 5, 3], np.uint32)
+    hbm, link, _ = bench.algorithmic_bytes(OFF, vals, 4, VB, RES, 4, "bfs", list_deg=3)
+    assert link == 0
+    assert hbm == 5 * 4 + 5 * 4 + 3 * (16 + 4)
+
+
+def test_whole_graph_algorithms_count_every_vertex_per_iteration(bench):
+    vals = np.zeros(4, np.uint32)
+    hbm, link, edges = bench.algorithmic_bytes(OFF, vals, 4, VB, RES, 4, "pr_push", n_iters=20)
+    assert link == 20 * 2 * 4
+    assert hbm == 20 * (3 * 4 + 5 * 8 + 4 * (16 + 4))
+    assert edges == 5
+
+
+def test_captured_traffic_scales_with_edges(bench):
+    t = bench.NCU_TRAFFIC["sssp"]
+    dram, sysmem = bench.traffic_for("sssp", 24, 2 * t["ne"])
+    assert dram == 2 * t["dram"] and sysmem == 2 * t["sysmem"]
+    assert bench.traffic_for("no-such-kernel", 24, 1) == (None, None)
