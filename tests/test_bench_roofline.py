@@ -53,3 +53,18 @@ def test_captured_traffic_scales_with_edges(bench):
     dram, sysmem = bench.traffic_for("sssp", 24, 2 * t["ne"])
     assert dram == 2 * t["dram"] and sysmem == 2 * t["sysmem"]
     assert bench.traffic_for("no-such-kernel", 24, 1) == (None, None)
+
+
+def test_union_find_bytes_skip_the_hub_component(bench):
+    # degrees 3, 1, 4, 0, 3; the hub (vertex 2) shares label 0 with vertices
+    # 0 and 1; vertices 3 and 4 are outside its component
+    off = np.array([0, 3, 4, 8, 8, 11], np.uint64)
+    labels = np.array([0, 0, 0, 3, 3], np.uint32)
+    vb = np.array([0, 3, 5], np.uint32)
+    res = np.array([True, False])
+    hbm, link, edges = bench.algorithmic_bytes_cc_uf(off, labels, 5, vb, res, 4, 0)
+    # sampled: min(deg, 2) = 2, 1, 2, 0, 2; the rest of a list only outside
+    # the hub's component (vertex 4: one more edge; vertex 0 skips its third)
+    assert edges == 2 + 1 + 2 + 0 + 3
+    assert link == (0 + 3) * 4                     # vertices 3, 4 are on the host
+    assert hbm == (2 + 1 + 2) * 4 + 8 * 8 + 5 * (16 + 12)
