@@ -1,16 +1,33 @@
 #!/usr/bin/env python
-"""Headline benchmark: GTEPS of the out-of-HBM frontier engine on one B200.
+"""Benchmarks of the out-of-HBM frontier engine on one B200, every config.
 
-Default workload (N=1): directed RMAT scale 24, edge factor 16 (a=.57,
-b=.19, c=.19), self-loops/duplicates removed, ids permuted, WCSR with
-weights in [1,64]; the HBM edge budget holds 40% of the edge bytes, the rest
-is read zero-copy from pinned host memory.  A step is one SSSP from source 1
-(bit-exact distances).  The second algorithm of the same configuration, CC
-(min-label propagation) on the symmetrised graph with the same 40% budget,
-is reported under "extra".
+Headline (the JSON line's value): config 2's SSSP.  Directed RMAT scale 24,
+edge factor 16 (a=.57, b=.19, c=.19), self-loops and duplicates removed, ids
+permuted, WCSR with weights in [1,64]; the HBM edge budget holds 40% of the
+edge bytes and the rest is read zero-copy from pinned host memory.  A step
+is one SSSP from source 1, bit-exact against the CPU oracle.
+
+The default N=1 run also measures every other config and reports each under
+"extra", each with its own parity check, clocks and (C1-C3) roofline:
+  c2_sssp_unpacked  the same SSSP with 8-byte {dst, w} edges (packing off),
+                    so 60% of the edges cross the host link as config 2 meant
+  c2_cc             CC by min-label propagation on the symmetrised graph,
+                    40% budget (the reference's method); c2_cc_union_find is
+                    the sampling union-find the engine uses by default on
+                    symmetric graphs (same labels)
+  c1_bfs            BFS, RMAT scale 20, fully resident, source 1
+  c3_pr_pull/push   PageRank on RMAT scale 26 (CSC / CSR), 2 GiB HBM edge
+                    budget, 20 iterations, every vertex within 1e-6 relative
+                    of the FP64 oracle
+  c4_bfs/c4_sssp    1,024 seeded sources on RMAT scale 26 in groups of 64
+                    vs single-source runs; the first group's 64 checksums
+                    equal those of single runs
+  c5                a short serving sweep (3 arrival rates) on RMAT scale 26,
+                    edge factor 48, served vs the same stream measured one
+                    query at a time; every answer equals its single run
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
-                  [--workload c2|c1|c3]
+                  [--workload c2|c1|c2cc|c3|c3push|c4|c5] [--no-extra]
 
 value: whole-job GTEPS = traversed edges (sum of out-degrees of the vertices
 the source reaches, each counted once) / device time, summed over ranks
@@ -36,28 +53,11 @@ sys.path.insert(0, ROOT)
 
 SEED = 0x54484592
 FALLBACK_HBM_GBS = 6650.0
-
-
-# DRAM and host-link (sysmem) bytes per launch of the dominant kernel, from the
-# ncu captures summarised in profiles/ (minq_sssp_rmat22_wcsr_packed_hbm40.md,
-# minprop_cc_rmat22_sym_hbm40.md, minprop_bfs_rmat20_resident.md,
-# pr_pull_rmat22_csc_hbm47.md).  Captures
-# made on a smaller graph are scaled to the bench size by edge count (the
-# traffic of these kernels grows with the edges traversed).
-NCU_TRAFFIC = {
-    "sssp": dict(scale=22, ne=65241959, dram=597834496 + 83409920, sysmem=3283365 * 32),
-    "cc": dict(scale=22, ne=128306542, dram=392704512 + 69563648, sysmem=11788847 * 32),
-    "bfs": dict(scale=20, ne=16084564, dram=41359616 + 613888, sysmem=0),
-    "pr_pull": dict(scale=22, ne=65241959, dram=135399168 + 20317184, sysmem=6104134 * 32, per="iteration"),
-}
-
-
-def traffic_for(algo, scale, ne, iters=1):
-    t = NCU_TRAFFIC.get(algo)
-    if not t:
-        return None, None
-    f = ne / t["ne"]
-    return int(t["dram"] * f * iters), int(t["sysmem"] * f * iters)
+PCIE_GEN5_X16_GBS = 64.0     # spec figure per direction, for context beside the measured link
+PR_RTOL = 1e-6               # PageRank: max per-vertex relative error vs the FP64 oracle
+TRAFFIC_TABLE = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+L2_NOTE = ("inputs larger than L2 (>= 64 MB of edges); the GPU arm also writes 256 MiB "
+           "between timed steps, outside the events")
 
 
 def peaks():
@@ -68,36 +68,74 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def parse():
+def measured_traffic(key):
+    """DRAM read+write bytes and host-link read bytes per launch of the
+    dominant kernel, from an ncu capture of exactly this workload (the
+    table in profiles/ncu_traffic.json, each entry with its command);
+    (None, None, None) when this workload was not captured."""
+    try:
+        table = json.load(open(TRAFFIC_TABLE))
+    except (OSError, ValueError):
+        return None, None, None
+    e = table.get(key)
+    if not e:
+        return None, None, None
+    return (int(e["dram_read_bytes"] + e["dram_write_bytes"]),
+            int(e["sysmem_read_sectors"] * 32) if e.get("sysmem_read_sectors") is not None else None,
+            e)
+
+
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c2cc", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2",
+                    choices=["c1", "c2", "c2cc", "c3", "c3push", "c4", "c5"])
     ap.add_argument("--edge-factor", type=int, default=0, help="override the edge factor")
     ap.add_argument("--rates", default="", help="c5: comma-separated arrival rates (queries/s)")
     ap.add_argument("--sssp-delta", type=int, default=0, help="c4: batched SSSP window width")
-    ap.add_argument("--queries", type=int, default=1024, help="c4: batched sources")
-    ap.add_argument("--plain-sample", type=int, default=16, help="c4: single-source runs timed")
+    ap.add_argument("--queries", type=int, default=0,
+                    help="c4: batched sources (default 1024); c5: queries per rate (default 96)")
     ap.add_argument("--group-min", type=int, default=0,
                     help="c5: queue depth from which the server runs batched groups (0 = default)")
     ap.add_argument("--scale", type=int, default=0, help="override the workload's scale")
     ap.add_argument("--source", type=int, default=1, help="BFS/SSSP source vertex")
     ap.add_argument("--budget-frac", type=float, default=-1.0,
                     help="override the HBM edge budget as a fraction of edge bytes")
-    ap.add_argument("--no-extra", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="headline workload only")
+    ap.add_argument("--only", default="", help="comma-separated extra sections to run")
     ap.add_argument("--no-cpu", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--time-guard-s", type=float, default=600.0,
+                    help="skip the remaining extra sections once the run is this old")
+    return ap.parse_args(argv)
 
 
 WORKLOADS = {
-    # name: (algo, scale, edge_factor, fmt, symmetric, budget_frac, budget_bytes)
     "c1": dict(algo="bfs", scale=20, ef=16, fmt="csr", sym=False, frac=1.0),
     "c2": dict(algo="sssp", scale=24, ef=16, fmt="wcsr", sym=False, frac=0.4),
     "c2cc": dict(algo="cc", scale=24, ef=16, fmt="csr", sym=True, frac=0.4),
     "c3": dict(algo="pr_pull", scale=26, ef=16, fmt="csc", sym=False, budget=2 << 30),
+    "c3push": dict(algo="pr_push", scale=26, ef=16, fmt="csr", sym=False, budget=2 << 30),
 }
+
+
+def budget_desc(wl):
+    if "budget" in wl:
+        return f"{wl['budget']} bytes"
+    return f"{int(round(wl['frac'] * 100))}% of the format's edge bytes"
+
+
+def workload_config(wl, source, gpus):
+    """The config dict both arms print (keys that describe the workload only)."""
+    return {"workload": f"{wl['algo']} rmat{wl['scale']} ef{wl['ef']} {wl['fmt']} "
+                        f"hbm-budget {budget_desc(wl)}",
+            "scale": wl["scale"], "edge_factor": wl["ef"], "format": wl["fmt"],
+            "symmetric": wl["sym"], "hbm_edge_budget": budget_desc(wl),
+            "source": source if wl["algo"] in ("bfs", "sssp") else None,
+            "pr_iterations": 20 if wl["algo"].startswith("pr") else None,
+            "parallelism": f"replicas x{gpus}", "l2": L2_NOTE}
 
 
 class Dist:
@@ -151,6 +189,7 @@ class Clocks:
             time.sleep(0.3)
         except OSError:
             self.proc = None
+        return self
 
     def stop(self):
         if not self.proc:
@@ -230,39 +269,112 @@ def algorithmic_bytes_cc_uf(off, labels, nv, vb, res, esz, list_deg):
     return hbm, link, int(edges_v.sum())
 
 
-def run_ours(args, dist):
-    import torch
-    import thievory_b200 as T
-    from oracle import oracle as O
-
-    dev = dist.local
-    torch.cuda.set_device(dev)
-    T.load_library()
-    hbm_peak, peak_kind = peaks()
-    wl = dict(WORKLOADS[args.workload])
-    if args.scale:
-        wl["scale"] = args.scale
-    if args.budget_frac >= 0:
-        wl.pop("budget", None)
-        wl["frac"] = args.budget_frac
-
-    link_mc, link_zc = T.link_bandwidth(dev, 1 << 30)
+def roofline(b_hbm, b_link, kern_s, hbm_peak, peak_kind, link_mc, link_zc, traffic_key,
+             launches_per_step, extra=None):
+    """Mixed HBM + host-link roofline of one step: T_roof = B_hbm/HBM + B_link/link."""
     link_peak = max(link_mc, link_zc)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
-    stream = torch.cuda.Stream(device=dev)
+    t_roof = b_hbm / (hbm_peak * 1e9) + b_link / (link_peak * 1e9)
+    t_spec = b_hbm / (hbm_peak * 1e9) + b_link / (PCIE_GEN5_X16_GBS * 1e9)
+    dram, link_t, entry = measured_traffic(traffic_key)
+    per = max(int(launches_per_step), 1)
+    r = {"bound": "hbm", "unit": "GB/s",
+         "achieved": (b_hbm + b_link) / kern_s / 1e9,
+         "peak": (b_hbm + b_link) / t_roof / 1e9,
+         "frac": t_roof / kern_s,
+         "frac_vs_pcie_gen5_spec": t_spec / kern_s,
+         "traffic": None if dram is None else dram * (entry.get("launches_per_step", 1)),
+         "link_traffic": None if link_t is None else link_t * (entry.get("launches_per_step", 1)),
+         "traffic_source": (f"ncu capture of this workload: {entry['command']}" if entry else
+                            "not captured at this size (null)"),
+         "algorithmic_hbm_bytes": b_hbm, "algorithmic_link_bytes": b_link,
+         "hbm_peak_gbs": hbm_peak, "hbm_peak_kind": peak_kind,
+         "link_peak_gbs": link_peak, "link_memcpy_gbs": link_mc, "link_zerocopy_gbs": link_zc,
+         "pcie_gen5_x16_spec_gbs": PCIE_GEN5_X16_GBS,
+         "kernel_ms": kern_s * 1e3, "launches_per_step": per,
+         "note": ("mixed bound: peak = bytes / (B_hbm/HBM + B_link/link), with HBM of measured "
+                  "and the link's measured pinned-memcpy or zero-copy rate; frac = T_roof / T")}
+    if extra:
+        r.update(extra)
+    return r
 
-    def measure(wl, k, w, want_e2e, want_cpu, run_kw=None):
-        run_kw = dict(run_kw or {})
-        g = T.Graph.generate_rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"],
-                                  fmt=wl["fmt"], device=dev)
-        budget = wl.get("budget", int(wl.get("frac", 1.0) * g.ne * g.esz))
-        algo = wl["algo"]
+
+class Bench:
+    """Per-process state shared by the measurements: device, stream, L2
+    flush buffer, peaks and the host-link rates."""
+
+    def __init__(self, args, dist):
+        import torch
+        import thievory_b200 as T
+
+        self.torch, self.T, self.args, self.dist = torch, T, args, dist
+        self.dev = dist.local
+        torch.cuda.set_device(self.dev)
+        T.load_library()
+        self.hbm_peak, self.peak_kind = peaks()
+        self.link_mc, self.link_zc = T.link_bandwidth(self.dev, 1 << 30)
+        self.flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{self.dev}")
+        self.stream = torch.cuda.Stream(device=self.dev)
+        self.sptr = self.stream.cuda_stream
+        self.t_start = time.perf_counter()
+
+    def gen(self, wl):
+        return self.T.Graph.generate_rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"],
+                                          fmt=wl["fmt"], device=self.dev)
+
+    @staticmethod
+    def plan(g, wl, algo=None):
+        algo = algo or wl["algo"]
+        budget = wl["budget"] if "budget" in wl else int(wl["frac"] * g.ne * g.esz)
         # PageRank reads whole blocks: no small-list cache
-        plan = g.plan(budget, small_list_degree=1 if algo.startswith("pr") else 0)
-        src = args.source
-        sptr = stream.cuda_stream
+        return budget, g.plan(budget, small_list_degree=1 if algo.startswith("pr") else 0)
+
+    def timed(self, g, algo, k, w, run_kw):
+        """w warm-up runs, then k runs each bracketed by CUDA events on the
+        launching stream, a 256 MiB write between them (outside the events),
+        clocks sampled throughout, barrier + synchronize on both sides."""
+        torch, dist = self.torch, self.dist
         for _ in range(w):
-            g.run(algo, source=src, want_values=False, stream=sptr, **run_kw)
+            g.run(algo, source=self.args.source, want_values=False, stream=self.sptr, **run_kw)
+        ck = Clocks(self.dev).start()
+        dist.barrier()
+        torch.cuda.synchronize(self.dev)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(k)]
+        lib_ms, launches, link_bytes, hbm_bytes = [], 0, 0, 0
+        with torch.cuda.stream(self.stream):
+            for i in range(k):
+                self.flush.zero_()
+                ev[i][0].record(self.stream)
+                _, st = g.run(algo, source=self.args.source, want_values=False, stream=self.sptr,
+                              **run_kw)
+                ev[i][1].record(self.stream)
+                lib_ms.append(st["device_ms"])
+                launches += st["kernel_launches"]
+                link_bytes += st["link_edge_bytes"]
+                hbm_bytes += st["hbm_edge_bytes"]
+        self.stream.synchronize()
+        dist.barrier()
+        clocks = ck.stop()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        total_s = dist.max(sum(step_ms) / 1e3)
+        return {"total_s": total_s, "step_ms": step_ms, "lib_ms": lib_ms, "launches": launches,
+                "link_bytes": link_bytes // k, "hbm_bytes": hbm_bytes // k, "clocks": clocks,
+                "k": k}
+
+    def measure(self, wl, k, w, want_e2e=False, cpu=True, run_kw=None, traffic_key=None,
+                graph=None, keep=False, label=""):
+        """One single-source / whole-graph workload: timing, roofline, the
+        oracle's answer on the host (checked equal; its time is the CPU
+        baseline), optionally e2e through the C ABI."""
+        from oracle import oracle as O
+
+        T, dist, args = self.T, self.dist, self.args
+        run_kw = dict(run_kw or {})
+        g = graph or self.gen(wl)
+        algo = wl["algo"]
+        budget, plan = self.plan(g, wl)
+        src = args.source
+        tm = self.timed(g, algo, k, w, run_kw)
         vals = g.values(algo)
         off, edges, outdeg = g.host_arrays()
         vb, res = g.blocks()
@@ -276,62 +388,30 @@ def run_ours(args, dist):
                                                     g.nv, vb, res, g.mem_esz, algo, iters, lcd)
         if algo == "cc" or algo.startswith("pr"):
             trav = g.ne * iters  # edges of the graph, however many were read
-        clocks = Clocks(dev)
-        clocks.start()
-        dist.barrier()
-        torch.cuda.synchronize(dev)
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(k)]
-        lib_ms, launches, link_bytes, hbm_bytes = [], 0, 0, 0
-        with torch.cuda.stream(stream):
-            for i in range(k):
-                flush.zero_()  # > L2 write between steps (outside the events)
-                ev[i][0].record(stream)
-                _, st = g.run(algo, source=src, want_values=False, stream=sptr, **run_kw)
-                ev[i][1].record(stream)
-                lib_ms.append(st["device_ms"])
-                launches += st["kernel_launches"]
-                link_bytes += st["link_edge_bytes"]
-                hbm_bytes += st["hbm_edge_bytes"]
-        stream.synchronize()
-        dist.barrier()
-        ck = clocks.stop()
-        step_ms = [a.elapsed_time(b) for a, b in ev]
-        total_s = dist.max(sum(step_ms) / 1e3)
-        value = dist.n * trav * k / total_s / 1e9
-        t_roof = b_hbm / (hbm_peak * 1e9) + b_link / (link_peak * 1e9)
-        kern_s = statistics.mean(lib_ms) / 1e3
-        # the captured CC kernel is label propagation's; union-find has its own
-        dram_t, link_t = traffic_for("cc_uf" if union_find else algo, wl["scale"], g.ne, iters)
+        kern_s = statistics.mean(tm["lib_ms"]) / 1e3
         out = {
-            "value": value, "ms_per_step": total_s * 1e3 / k, "traversed_edges": trav,
-            "plan": plan, "clocks": ck, "gpu_launches": launches,
+            "value": dist.n * trav * tm["k"] / tm["total_s"] / 1e9, "unit": "GTEPS",
+            "ms_per_step": tm["total_s"] * 1e3 / tm["k"], "steps": tm["k"], "warmup": w,
+            "traversed_edges": trav, "clocks": tm["clocks"],
+            "gpu_launches": tm["launches"],
+            "plan": {k_: plan[k_] for k_ in ("num_blocks", "resident_blocks", "resident_edge_bytes",
+                                             "host_edge_bytes", "small_list_degree",
+                                             "small_list_bytes", "small_list_vertices")},
             "storage": {"format_edge_bytes": g.esz, "stored_edge_bytes": g.mem_esz,
                         "packed_weight_bits": g.weight_bits, "budget_bytes": budget},
-            "roofline": {
-                "bound": "hbm", "unit": "GB/s",
-                "achieved": (b_hbm + b_link) / kern_s / 1e9,
-                "peak": (b_hbm + b_link) / t_roof / 1e9,
-                "frac": t_roof / kern_s,
-                "traffic": dram_t, "link_traffic": link_t,
-                "traffic_note": "dram read+write (and host-link sysmem sectors) per launch from an "
-                                "ncu capture, scaled by edge count when captured on a smaller graph",
-                "algorithmic_hbm_bytes": b_hbm, "algorithmic_link_bytes": b_link,
-                "hbm_peak_gbs": hbm_peak, "hbm_peak_kind": peak_kind,
-                "link_peak_gbs": link_peak, "link_memcpy_gbs": link_mc, "link_zerocopy_gbs": link_zc,
-                "kernel_ms": kern_s * 1e3,
-                "actual_link_bytes_per_step": link_bytes // k,
-                "actual_hbm_edge_bytes_per_step": hbm_bytes // k,
-                "note": "mixed bound: peak = bytes / (B_hbm/HBM + B_link/link); frac = T_roof / T",
-            },
+            "roofline": roofline(b_hbm, b_link, kern_s, self.hbm_peak, self.peak_kind, self.link_mc,
+                                 self.link_zc, traffic_key, tm["launches"] / tm["k"],
+                                 {"actual_link_bytes_per_step": tm["link_bytes"],
+                                  "actual_hbm_edge_bytes_per_step": tm["hbm_bytes"]}),
         }
         if want_e2e:
-            host = torch.empty(g.nv * (2 if algo.startswith("pr") else 1), dtype=torch.int32).pin_memory()
+            host = self.torch.empty(g.nv * (2 if algo.startswith("pr") else 1),
+                                    dtype=self.torch.int32).pin_memory()
             hv = host.numpy().view(np.float64 if algo.startswith("pr") else np.uint32)
             wall = []
             for _ in range(k):
                 t0 = time.perf_counter()
-                _, st = g.run(algo, source=src, out=hv, stream=sptr, **run_kw)
+                _, st = g.run(algo, source=src, out=hv, stream=self.sptr, **run_kw)
                 wall.append(time.perf_counter() - t0)
             tw = dist.max(sum(wall))
             out["e2e"] = {"value": dist.n * trav * k / tw / 1e9, "unit": "GTEPS",
@@ -340,184 +420,307 @@ def run_ours(args, dist):
                           "note": "h2d = zero-copy edge bytes read over the host link"}
             if algo in ("bfs", "sssp", "cc"):
                 assert np.array_equal(hv, vals), "e2e values differ from device run"
-        if want_cpu and dist.rank == 0 and dist.n == 1:
+        if cpu and dist.rank == 0 and dist.n == 1:
             L = O.lib()
-            cv = np.empty(g.nv, np.uint32)
-            P = lambda a: None if a is None else a.ctypes.data
+            P = lambda a: None if a is None else a.ctypes.data  # noqa: E731
             t0 = time.perf_counter()
-            if algo == "sssp":
-                L.thvo_sssp_par(g.nv, P(off), P(edges), None, 2, src, P(cv))
-            elif algo == "bfs":
-                L.thvo_bfs_par(g.nv, P(off), P(edges), 1, src, P(cv))
-            elif algo == "cc":
-                L.thvo_cc_par(g.nv, P(off), P(edges), 1, P(cv))
-            elif algo == "pr_pull":
-                # bounded sample: 2 of the 20 iterations, checked against the
-                # GPU run of the same 2 iterations
-                pr_cpu = np.empty(g.nv, np.float64)
-                L.thvo_pagerank_csc(g.nv, P(off), P(edges), P(outdeg), 2, 0.85, P(pr_cpu))
-            dt = time.perf_counter() - t0
-            sample = f"one full {algo} run of this workload on the host"
-            work = trav
             if algo in ("bfs", "sssp", "cc"):
-                assert np.array_equal(cv, vals), "GPU result differs from the CPU oracle"
-            elif algo == "pr_pull":
-                gpu2, _ = g.run(algo, pr_iters=2, stream=sptr)
-                assert np.max(np.abs(gpu2 - pr_cpu) / np.abs(pr_cpu)) <= 1e-6, "PageRank differs"
-                work = 2 * g.ne
-                sample = "2 PageRank iterations of this workload on the host"
-            out["cpu_baseline"] = {"value": work / dt / 1e9, "unit": "GTEPS", "cores": O.threads(),
+                cv = np.empty(g.nv, np.uint32)
+                if algo == "sssp":
+                    L.thvo_sssp_par(g.nv, P(off), P(edges), None, 2, src, P(cv))
+                elif algo == "bfs":
+                    L.thvo_bfs_par(g.nv, P(off), P(edges), 1, src, P(cv))
+                else:
+                    L.thvo_cc_par(g.nv, P(off), P(edges), 1, P(cv))
+                dt = time.perf_counter() - t0
+                assert np.array_equal(cv, vals), f"{label or algo}: GPU result differs from the CPU oracle"
+                out["check"] = (f"all {g.nv} values bit-exact vs the CPU oracle "
+                                f"({'Dijkstra-equivalent label-correcting' if algo == 'sssp' else algo})")
+                out["oracle_values"] = cv
+            else:
+                # the FP64 oracle over the in-edges (CSC); a CSR graph's is
+                # supplied by the caller (the transpose of the same graph)
+                cv = np.empty(g.nv, np.float64)
+                L.thvo_pagerank_csc(g.nv, P(off), P(edges), P(outdeg), 20, 0.85, P(cv))
+                dt = time.perf_counter() - t0
+                out["oracle_values"] = cv
+            out["cpu_baseline"] = {"value": trav / dt / 1e9, "unit": "GTEPS", "cores": O.threads(),
                                    "kind": "port",
-                                   "sample": f"{sample} (OpenMP oracle, {dt:.2f} s); "
-                                             "result checked equal"}
-        g.close()
+                                   "sample": f"one full run of this workload on the host "
+                                             f"(OpenMP oracle, {dt:.2f} s)"}
+        out["values"] = vals
+        if keep:
+            out["graph"] = g
+        elif graph is None:
+            g.close()
         return out
 
-    main = measure(wl, args.steps, args.warmup, True, not args.no_cpu)
+    def elapsed(self):
+        return time.perf_counter() - self.t_start
+
+
+def public(d, drop=("values", "oracle_values", "graph")):
+    return {k: v for k, v in d.items() if k not in drop}
+
+
+def pr_check(gpu, ref, label):
+    rel = float(np.max(np.abs(gpu - ref) / np.abs(ref)))
+    assert rel <= PR_RTOL, f"{label}: PageRank max relative error {rel:.3e} > {PR_RTOL}"
+    return rel
+
+
+def run_headline(b, args):
+    """Config 2 SSSP (the line's value) and, with extras, the rest of config 2."""
+    wl = dict(WORKLOADS[args.workload])
+    if args.scale:
+        wl["scale"] = args.scale
+    if args.budget_frac >= 0:
+        wl.pop("budget", None)
+        wl["frac"] = args.budget_frac
+    key = f"{wl['algo']}_rmat{wl['scale']}_{wl['fmt']}_{budget_desc(wl).split()[0]}"
+    keep = args.workload == "c2" and not args.no_extra and b.dist.world == 1
+    main = b.measure(wl, args.steps, args.warmup, want_e2e=True, cpu=not args.no_cpu,
+                     traffic_key=key, keep=keep)
+    if wl["algo"] in ("pr_pull",) and "oracle_values" in main:
+        main["check"] = (f"all {len(main['values'])} ranks within "
+                         f"{pr_check(main['values'], main['oracle_values'], 'pagerank'):.2e} "
+                         f"relative of the FP64 oracle (tolerance {PR_RTOL})")
     extra = {}
-    if args.workload == "c2" and not args.no_extra:
-        cc = measure(dict(WORKLOADS["c2cc"], scale=wl["scale"]), args.steps, args.warmup, False,
-                     not args.no_cpu)
-        extra["cc_rmat_sym_40pct"] = {k: cc[k] for k in ("value", "ms_per_step", "traversed_edges",
-                                                          "roofline", "gpu_launches")}
-        extra["cc_rmat_sym_40pct"]["algorithm"] = ("sampling union-find (the graph is symmetric): "
-                                                   "same labels as min-label propagation")
-        if "cpu_baseline" in cc:
-            extra["cc_rmat_sym_40pct"]["cpu_baseline"] = cc["cpu_baseline"]
-        lp = measure(dict(WORKLOADS["c2cc"], scale=wl["scale"]), args.steps, args.warmup, False,
-                     False, {"label_propagation": True})
-        extra["cc_rmat_sym_40pct_label_propagation"] = {
-            k: lp[k] for k in ("value", "ms_per_step", "traversed_edges", "roofline", "gpu_launches")}
+    if keep:
+        g = main.pop("graph")
+        ref_vals = main.get("oracle_values", main["values"])
+        # config 2 as it was meant: 8-byte {dst, w} edges, 40% of them resident
+        g.set_edge_packing(False)
+        up = b.measure(wl, max(3, args.steps // 2), 3, cpu=False, graph=g,
+                       traffic_key=key + "_unpacked")
+        assert np.array_equal(up["values"], ref_vals), "unpacked SSSP differs"
+        up["check"] = "all values bit-exact vs the packed run (itself checked vs the CPU oracle)"
+        extra["c2_sssp_unpacked"] = public(up)
+        g.close()
+        # CC: min-label propagation is the reference's method (the CC figure);
+        # union-find is the engine's default on symmetric graphs
+        wcc = dict(WORKLOADS["c2cc"], scale=wl["scale"])
+        gcc = b.gen(wcc)
+        lp = b.measure(wcc, args.steps, args.warmup, cpu=not args.no_cpu,
+                       run_kw={"label_propagation": True}, graph=gcc,
+                       traffic_key=f"cc_lp_rmat{wl['scale']}_sym_40%", label="cc label propagation")
+        lp["algorithm"] = "min-label propagation (the reference's CC method)"
+        extra["c2_cc"] = public(lp)
+        uf = b.measure(wcc, args.steps, args.warmup, cpu=False, graph=gcc,
+                       traffic_key=f"cc_uf_rmat{wl['scale']}_sym_40%")
+        if "oracle_values" in lp:
+            assert np.array_equal(uf["values"], lp["oracle_values"]), "union-find CC differs"
+            uf["check"] = "all labels bit-exact vs the CPU oracle (min-label fixed point)"
+        uf["algorithm"] = ("sampling union-find (the graph is symmetric): same labels as min-label "
+                           "propagation, reads 3% of the edges; GTEPS counts every edge")
+        extra["c2_cc_union_find"] = public(uf)
+        gcc.close()
     return wl, main, extra
 
 
-def run_batched(args, dist):
-    """Config 4: 1,024 seeded sources over the non-isolated vertices, batched
-    in groups of 64 (one persistent launch per group) vs single-source runs
-    of a sample of the same sources; per-source checksums of the sample must
-    match the batched ones bit for bit."""
-    import torch
-    import thievory_b200 as T
+def run_c1(b, args):
+    wl = dict(WORKLOADS["c1"])
+    m = b.measure(wl, args.steps, args.warmup, want_e2e=True, cpu=not args.no_cpu,
+                  traffic_key="bfs_rmat20_csr_100%")
+    m["config"] = workload_config(wl, args.source, args.gpus)
+    return public(m)
 
-    dev = dist.local
-    torch.cuda.set_device(dev)
-    T.load_library()
-    scale = args.scale or 26
-    budget = 2 << 30 if args.budget_frac < 0 else None
+
+def run_c3(b, args):
+    """PageRank pull (CSC) and push (CSR), 20 iterations, both checked at
+    every vertex against one FP64 oracle run over the CSC (the CSR is the
+    same graph: the generator builds the CSC as its transpose)."""
+    k, w = min(args.steps, 3), 3
+    out = {}
+    wl = dict(WORKLOADS["c3"])
+    pull = b.measure(wl, k, w, cpu=not args.no_cpu, traffic_key="pr_pull_rmat26_csc_2GiB")
+    ref = pull.pop("oracle_values", None)
+    if ref is not None:
+        pull["check"] = (f"all {len(ref)} ranks after 20 iterations within "
+                         f"{pr_check(pull['values'], ref, 'pr_pull'):.2e} relative of the FP64 "
+                         f"oracle (tolerance {PR_RTOL})")
+    pull["config"] = workload_config(wl, None, args.gpus)
+    out["c3_pr_pull"] = public(pull)
+    wl = dict(WORKLOADS["c3push"])
+    push = b.measure(wl, k, w, cpu=False, traffic_key="pr_push_rmat26_csr_2GiB", keep=True)
+    if ref is not None:
+        push["check"] = (f"all {len(ref)} ranks after 20 iterations within "
+                         f"{pr_check(push['values'], ref, 'pr_push'):.2e} relative of the FP64 "
+                         f"oracle (tolerance {PR_RTOL})")
+        push["cpu_baseline"] = dict(pull["cpu_baseline"],
+                                    sample=pull["cpu_baseline"]["sample"] + "; the same oracle run "
+                                    "(pull over the CSC) gives the push ranks")
+    push["config"] = workload_config(wl, None, args.gpus)
+    g = push.pop("graph")
+    out["c3_pr_push"] = public(push)
+    return out, g
+
+
+def run_c4(b, args, g_csr=None):
+    """Config 4: 1,024 seeded sources over the non-isolated vertices of
+    RMAT scale 26, batched in groups of 64 (one persistent, graph-captured
+    launch per group) vs single-source runs of the first group's 64 sources,
+    whose checksums must equal the batched ones bit for bit."""
+    T = b.T
+    scale = args.scale if args.workload == "c4" and args.scale else 26
+    n = args.queries or 1024
     out = {}
     for algo, fmt in (("bfs", "csr"), ("sssp", "wcsr")):
-        g = T.Graph.generate_rmat(scale, 16, seed=SEED, fmt=fmt, device=dev)
-        g.plan(budget if budget is not None else int(args.budget_frac * g.ne * g.esz))
-        src = g.pick_sources(args.queries, SEED)
+        g = g_csr if (algo == "bfs" and g_csr is not None and scale == 26) else \
+            T.Graph.generate_rmat(scale, 16, seed=SEED, fmt=fmt, device=b.dev)
+        budget = 2 << 30 if args.budget_frac < 0 else int(args.budget_frac * g.ne * g.esz)
+        plan = g.plan(budget)
+        src = g.pick_sources(n, SEED)
         dl = args.sssp_delta if algo == "sssp" else 0
         g.batch_run(algo, src[:64], want_values=False, sssp_delta=dl, tune=True)  # tunes, warms up
+        ck = Clocks(b.dev).start()
         _, sums, bst = g.batch_run(algo, src, want_values=False, sssp_delta=dl, tune=True)
+        clocks = ck.stop()
+        nplain = min(64, n)
         plain_ms, plain_bytes = [], []
-        for s_ in src[: args.plain_sample]:
-            vals, st = g.run(algo, source=int(s_))
+        for i, s_ in enumerate(src[:nplain]):
+            _, st = g.run(algo, source=int(s_), want_values=False, checksum=True)
             plain_ms.append(st["device_ms"])
             plain_bytes.append(st["hbm_edge_bytes"] + st["link_edge_bytes"])
-            i = int(np.nonzero(src == s_)[0][0])
-            assert T.values_checksum(vals) == int(sums[i]), f"{algo} source {s_} differs"
-        qps_b = dist.n * len(src) / (dist.max(bst["device_ms"]) / 1e3)
-        qps_p = dist.n * 1e3 / dist.max(statistics.mean(plain_ms))
-        out[algo] = {"batched_qps": qps_b, "plain_qps": qps_p, "speedup": qps_b / qps_p,
-                     "sssp_delta": dl,
-                     "batched_ms_total": bst["device_ms"], "plain_ms_mean": statistics.mean(plain_ms),
-                     "queries": len(src), "plain_sample": args.plain_sample,
-                     "batched_link_bytes": bst["link_edge_bytes"], "batched_iterations": bst["iterations"],
-                     # edge bytes read: all groups together vs the plain form
-                     # (sampled mean per query x queries)
-                     "batched_edge_bytes": bst["hbm_edge_bytes"] + bst["link_edge_bytes"],
-                     "plain_form_edge_bytes": statistics.mean(plain_bytes) * len(src),
-                     "checked": f"{args.plain_sample} sources: single-run checksum == batched checksum"}
+            assert st["checksum"] == int(sums[i]), f"c4 {algo} source {s_} differs"
+        qps_b = b.dist.n * len(src) / (b.dist.max(bst["device_ms"]) / 1e3)
+        qps_p = b.dist.n * 1e3 / b.dist.max(statistics.mean(plain_ms))
+        out[f"c4_{algo}"] = {
+            "batched_qps": qps_b, "plain_qps": qps_p, "speedup": qps_b / qps_p,
+            "sssp_delta": dl, "batched_ms_total": bst["device_ms"],
+            "plain_ms_mean": statistics.mean(plain_ms), "queries": len(src),
+            "groups": (len(src) + 63) // 64, "batched_iterations": bst["iterations"],
+            "batched_launches": bst["kernel_launches"],
+            "batched_link_bytes": bst["link_edge_bytes"],
+            "batched_edge_bytes": bst["hbm_edge_bytes"] + bst["link_edge_bytes"],
+            "plain_form_edge_bytes": statistics.mean(plain_bytes) * len(src),
+            "clocks": clocks,
+            "config": {"workload": f"{algo} rmat{scale} ef16 {fmt}, HBM edge budget {budget} bytes, "
+                                   f"{len(src)} seeded sources, groups of 64",
+                       "resident_edge_bytes": plan["resident_edge_bytes"],
+                       "host_edge_bytes": plan["host_edge_bytes"]},
+            "check": (f"the first group's {nplain} sources: single-run checksum == batched checksum "
+                      f"(sum over v of splitmix64(v<<32|value))"),
+            "timing": "batched: device time of all groups (CUDA events); plain: mean device time "
+                      "of the single runs"}
         g.close()
-    return scale, out
+    return out
 
 
-def run_serving(args, dist):
-    """Config 5 (scaled to the box): a Poisson stream, 80% BFS / 20% SSSP,
-    sources uniform over non-isolated vertices, served by continuous batching
-    vs the same stream run one query at a time with the plain kernels (FIFO
-    replay of measured single-query device times on the same arrivals).
-    Every served query's checksum must equal its plain run's."""
-    import torch
-    import thievory_b200 as T
+def stream_plain(g, algos, src, arr):
+    """The stream run one query at a time on the plain kernels: each query
+    starts at its arrival or when the previous one finishes; host wall
+    clock, as the server's latencies."""
+    t0 = time.perf_counter()
+    lat, sums = [], []
+    for i, (a, s_) in enumerate(zip(algos, src)):
+        target = t0 + arr[i] - arr[0]
+        d = target - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        _, st = g.run(a, source=int(s_), want_values=False, checksum=True)
+        lat.append(time.perf_counter() - target)
+        sums.append(st["checksum"])
+    return len(src) / (time.perf_counter() - t0), np.array(lat) * 1e3, sums
 
-    dev = dist.local
-    torch.cuda.set_device(dev)
-    T.load_library()
-    scale = args.scale or 26
+
+def stream_served(T, g, algos, src, arr, group_min):
+    with T.Server(g, max_slots=64, group_min=group_min) as sv:
+        t0 = time.perf_counter()
+        tickets = []
+        for i, (a, s_) in enumerate(zip(algos, src)):
+            d = t0 + arr[i] - arr[0] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(sv.submit(a, int(s_), want_values=False))
+        stats = [sv.wait(t, timeout_ms=600000)[1] for t in tickets]
+        t1 = time.perf_counter()
+    return len(src) / (t1 - t0), stats
+
+
+def run_c5(b, args):
+    """Config 5 (scaled to the box; the scale-30 graph needs ~206 GB CSR
+    of pinned host memory): a Poisson stream, 80% BFS / 20% SSSP, sources
+    uniform over non-isolated vertices, served with continuous batching vs
+    the same stream measured one query at a time on the plain kernels.
+    Every served answer's checksum equals the plain run's."""
+    T = b.T
+    scale = args.scale if args.workload == "c5" and args.scale else 26
     ef = args.edge_factor or 48
     frac = args.budget_frac if args.budget_frac >= 0 else 0.58
-    g = T.Graph.generate_rmat(scale, ef, seed=SEED, fmt="wcsr", device=dev)
+    n = args.queries or 96
+    g = T.Graph.generate_rmat(scale, ef, seed=SEED, fmt="wcsr", device=b.dev)
     # HBM budget: frac of the graph's CSR bytes (4 per edge), as ~120 GB of
     # the ~206 GB CSR at scale 30 / edge factor 48
     plan = g.plan(int(frac * g.ne * 4))
-    n = args.queries
     src = g.pick_sources(n, SEED)
     algos = ["sssp" if i % 5 == 0 else "bfs" for i in range(n)]
-    plain_ms, plain_sum = [], []
-    for a, s_ in zip(algos, src):
-        _, st = g.run(a, source=int(s_), want_values=False, checksum=True)
-        plain_ms.append(st["device_ms"])
-        plain_sum.append(st["checksum"])
-    # warm-up outside the timed sweep: tune the batched-group kernels the
-    # server uses for deep queues (cached in-process) and allocate their state
+    # warm-up outside the sweep: tune the batched-group kernels the server
+    # uses for deep queues (cached in-process) and allocate their state
     for a in ("bfs", "sssp"):
         g.batch_run(a, src[:64], want_values=False, tune=True)
+    probe = [g.run(a, source=int(s_), want_values=False)[1]["device_ms"]
+             for a, s_ in zip(algos[:10], src[:10])]
+    cap = 1e3 / statistics.mean(probe)  # plain capacity estimate, queries/s
+    rates = [float(x) for x in args.rates.split(",")] if args.rates else [cap, 4 * cap, 32 * cap]
     rng = np.random.default_rng(SEED)
-    rates = [float(x) for x in args.rates.split(",")] if args.rates else [
-        0.5 * 1e3 / statistics.mean(plain_ms), 4e3 / statistics.mean(plain_ms),
-        32e3 / statistics.mean(plain_ms)]
-    sweep = []
+    sweep, answers = [], None
+    ck = Clocks(b.dev).start()
     for rate in rates:
         arr = np.cumsum(rng.exponential(1.0 / rate, n))
-        # plain: FIFO replay of the measured service times on these arrivals
-        fin, lat = 0.0, []
-        for t_a, ms in zip(arr, plain_ms):
-            fin = max(fin, t_a) + ms / 1e3
-            lat.append(fin - t_a)
-        plain_qps = n / (fin - arr[0])
-        with T.Server(g, max_slots=64, group_min=args.group_min) as sv:
-            t0 = time.perf_counter()
-            tickets = []
-            for i, (a, s_) in enumerate(zip(algos, src)):
-                d = t0 + arr[i] - arr[0] - time.perf_counter()
-                if d > 0:
-                    time.sleep(d)
-                tickets.append(sv.submit(a, int(s_), want_values=False))
-            stats = [sv.wait(t, timeout_ms=600000)[1] for t in tickets]
-            t1 = time.perf_counter()
+        pq, plat, psum = stream_plain(g, algos, src, arr)
+        if answers is None:
+            answers = psum
+        assert psum == answers, "plain stream answers differ between rates"
+        sq, stats = stream_served(T, g, algos, src, arr, args.group_min)
         for i, st in enumerate(stats):
-            assert st["checksum"] == plain_sum[i], f"query {i} ({algos[i]} {src[i]}) differs"
+            assert st["checksum"] == answers[i], f"c5 query {i} ({algos[i]} {src[i]}) differs"
         slat = np.array([st["latency_ms"] for st in stats])
-        sweep.append({"rate_qps": rate, "served_qps": n / (t1 - t0),
+        modes = [st["grouped"] for st in stats]
+        joined = sum(st["joined"] for st in stats)
+        sweep.append({"rate_qps": rate, "served_qps": sq, "plain_qps": pq, "speedup": sq / pq,
                       "served_p50_ms": float(np.percentile(slat, 50)),
                       "served_p99_ms": float(np.percentile(slat, 99)),
-                      "plain_qps": plain_qps,
-                      "plain_p50_ms": float(np.percentile(np.array(lat) * 1e3, 50)),
-                      "plain_p99_ms": float(np.percentile(np.array(lat) * 1e3, 99))})
+                      "plain_p50_ms": float(np.percentile(plat, 50)),
+                      "plain_p99_ms": float(np.percentile(plat, 99)),
+                      "served_modes": {"slot": modes.count(0), "group": modes.count(1),
+                                       "alone": modes.count(2), "joined_while_running": joined}})
+    clocks = ck.stop()
     g.close()
-    return scale, ef, frac, plan, sweep, statistics.mean(plain_ms)
+    return {"sweep": sweep, "clocks": clocks, "queries_per_rate": n,
+            "plain_single_ms_probe": statistics.mean(probe),
+            "check": "every served answer's checksum == the plain run's (both streams, every rate)",
+            "timing": "host wall clock from the first arrival to the last answer; latency = answer - "
+                      "arrival; the plain stream is measured, one query at a time",
+            "config": {"workload": f"c5 serving rmat{scale} ef{ef} wcsr, HBM edge budget "
+                                   f"{int(round(frac * 100))}% of the CSR bytes, 80% BFS / 20% SSSP, "
+                                   f"{n} Poisson arrivals per rate",
+                       "resident_edge_bytes": plan["resident_edge_bytes"],
+                       "host_edge_bytes": plan["host_edge_bytes"]}}
 
 
 def run_reference(args, dist):
     """CPU oracle (the reference has no CPU path) on the same workload."""
     from oracle import oracle as O
 
-    wl = dict(WORKLOADS[args.workload])
+    wl = dict(WORKLOADS[args.workload if args.workload in WORKLOADS else "c2"])
     if args.scale:
         wl["scale"] = args.scale
+    if args.budget_frac >= 0:
+        wl.pop("budget", None)
+        wl["frac"] = args.budget_frac
     # all host cores: torchrun sets OMP_NUM_THREADS=1 for every rank, and
     # here rank 0 alone does the work
     O.set_threads(len(os.sched_getaffinity(0)))
     g = O.rmat(wl["scale"], wl["ef"], seed=SEED, symmetric=wl["sym"], weighted=wl["algo"] == "sssp")
     algo = wl["algo"]
+    if algo.startswith("pr"):
+        csc = O.transpose(g)
     fn = {"sssp": lambda: O.sssp(g, args.source, parallel=True),
           "bfs": lambda: O.bfs(g, args.source, parallel=True),
           "cc": lambda: O.cc(g, parallel=True),
-          "pr_pull": lambda: O.pagerank(g, 20)}[algo]
+          "pr_pull": lambda: O.pagerank_csc(*csc, 20),
+          "pr_push": lambda: O.pagerank_csc(*csc, 20)}[algo]
     for _ in range(args.warmup):
         vals = fn()
     t = []
@@ -540,79 +743,69 @@ def main():
         wl, value, ms, cores = run_reference(args, dist)
         line = {"metric": f"GTEPS ({wl['algo']})", "value": value, "unit": "GTEPS", "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-                "data": "synthetic (seeded RMAT, CPU generator)",
-                "config": {"workload": f"{wl['algo']} rmat{wl['scale']} ef{wl['ef']}"},
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32"
+                if not wl["algo"].startswith("pr") else "f64",
+                "data": "synthetic (seeded RMAT a=.57 b=.19 c=.19, dedup, no self-loops, permuted ids)",
+                "config": workload_config(wl, args.source, args.gpus),
                 "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": cores, "kind": "port",
-                                 "sample": f"full {wl['algo']} run per step on the host (OpenMP oracle)"},
+                                 "sample": f"one full {wl['algo']} run per step on the host (OpenMP "
+                                           f"oracle; the reference has no CPU implementation)"},
                 "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         dist.close()
         return
-    if args.workload == "c5":
-        scale, ef, frac, plan, sweep, plain_mean = run_serving(args, dist)
+    b = Bench(args, dist)
+    if args.workload in ("c4", "c5"):
+        out = run_c4(b, args) if args.workload == "c4" else run_c5(b, args)
         if dist.rank == 0:
-            top = max(sweep, key=lambda r: r["served_qps"])
-            line = {"metric": "queries/s served (continuous batching, 80% BFS / 20% SSSP)",
-                    "value": top["served_qps"], "unit": "queries/s", "n_gpus": args.gpus,
-                    "steps": args.queries, "warmup": 0, "ms_per_step": 1e3 / top["served_qps"],
-                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-                    "data": "synthetic (seeded RMAT, Poisson arrivals)",
-                    "config": {"workload": f"c5 serving rmat{scale} ef{ef} wcsr, HBM edge budget "
-                                           f"{int(frac * 100)}% of the CSR bytes, {args.queries} queries per rate",
-                               "resident_edge_bytes": plan["resident_edge_bytes"],
-                               "host_edge_bytes": plan["host_edge_bytes"],
-                               "small_list_cache": {k: plan[k] for k in (
-                                   "small_list_degree", "small_list_bytes", "small_list_vertices")}},
-                    "plain_mean_ms": plain_mean, "sweep": sweep}
-            print(json.dumps(line))
+            print(json.dumps({"workload": args.workload, "n_gpus": args.gpus, **out},
+                             default=float))
         dist.close()
         return
-    if args.workload == "c4":
-        scale, out = run_batched(args, dist)
-        if dist.rank == 0:
-            b = out["bfs"]
-            line = {"metric": "queries/s (batched 64-source BFS)", "value": b["batched_qps"],
-                    "unit": "queries/s", "n_gpus": args.gpus, "steps": 1, "warmup": 1,
-                    "ms_per_step": b["batched_ms_total"], "higher_is_better": True,
-                    "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-                    "data": "synthetic (seeded RMAT)",
-                    "config": {"workload": f"c4 batched BFS/SSSP rmat{scale} ef16, 2 GiB HBM edge budget, "
-                                           f"{args.queries} seeded sources, groups of 64"},
-                    "extra": out}
-            print(json.dumps(line))
-        dist.close()
-        return
-    wl, m, extra = run_ours(args, dist)
+    wl, m, extra = run_headline(b, args)
+    sections = ["c1", "c3", "c4", "c5"] if args.workload == "c2" and not args.no_extra else []
+    if args.only:
+        sections = [s for s in sections if s in args.only.split(",")]
+    if dist.world > 1:
+        sections = []  # replicas: the extra configs are measured at N=1
+    g_csr = None
+    for s in sections:
+        if b.elapsed() > args.time_guard_s:
+            extra[s] = {"skipped": f"time guard: the run was {b.elapsed():.0f} s old"}
+            continue
+        t0 = time.perf_counter()
+        if s == "c1":
+            extra["c1_bfs"] = run_c1(b, args)
+        elif s == "c3":
+            r, g_csr = run_c3(b, args)
+            extra.update(r)
+        elif s == "c4":
+            extra.update(run_c4(b, args, g_csr))
+            g_csr = None
+        elif s == "c5":
+            extra["c5"] = run_c5(b, args)
+        extra.setdefault("section_seconds", {})[s] = round(time.perf_counter() - t0, 1)
+    if g_csr is not None:
+        g_csr.close()
     if dist.rank == 0:
-        budget_desc = (f"{int(wl['frac'] * 100)}% of the format's edge bytes" if "frac" in wl
-                       else f"{wl['budget']} bytes")
         line = {
             "metric": f"GTEPS ({wl['algo']})", "value": m["value"], "unit": "GTEPS",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32",
+            "vs_baseline": None, "dtype": "u32" if not wl["algo"].startswith("pr") else "f32",
             "data": "synthetic (seeded RMAT a=.57 b=.19 c=.19, dedup, no self-loops, permuted ids)",
-            "config": {"workload": f"{wl['algo']} rmat{wl['scale']} ef{wl['ef']} {wl['fmt']} "
-                                   f"hbm-budget {budget_desc}",
-                       "scale": wl["scale"], "edge_factor": wl["ef"], "format": wl["fmt"],
-                       "hbm_edge_budget": budget_desc, "source": args.source,
-                       "resident_edge_bytes": m["plan"]["resident_edge_bytes"],
-                       "host_edge_bytes": m["plan"]["host_edge_bytes"],
-                       "small_list_cache": {k: m["plan"][k] for k in (
-                           "small_list_degree", "small_list_bytes", "small_list_vertices")},
-                       "edge_storage": m["storage"],
-                       "traversed_edges_per_step": m["traversed_edges"],
-                       "parallelism": f"replicas x{args.gpus}",
-                       "l2": "256 MiB device write between timed steps (outside the events)"},
+            "config": workload_config(wl, args.source, args.gpus),
+            "plan": m["plan"], "edge_storage": m["storage"],
+            "traversed_edges_per_step": m["traversed_edges"],
             "roofline": m["roofline"], "gpu_launches": m["gpu_launches"],
-            "clocks": m["clocks"], "e2e": m.get("e2e"),
+            "clocks": m["clocks"], "e2e": m.get("e2e"), "check": m.get("check"),
         }
         if "cpu_baseline" in m:
             line["cpu_baseline"] = m["cpu_baseline"]
         if extra:
             line["extra"] = extra
-        print(json.dumps(line))
+        line["run_seconds"] = round(b.elapsed(), 1)
+        print(json.dumps(line, default=float))
     dist.close()
 
 

@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define THV_ABI_VERSION 2
+#define THV_ABI_VERSION 3
 
 typedef enum thv_status {
   THV_OK = 0,
@@ -288,10 +288,15 @@ thv_status thv_batch_run(thv_graph *g, thv_algo algo, const uint32_t *sources,
 
 /* ---- serving (continuous batching) ---- */
 /* A server owns the graph while it runs (no other thv_run on it meanwhile).
- * Queries occupy slots of one resident traversal: a query that arrives while
- * others run is admitted at the next iteration boundary where a slot and its
- * memory are free, and its iterations overlap theirs on the device.  Results
- * are bit-identical to thv_run of the same source. */
+ * By default queries run in batched groups, one per algorithm, that stay on
+ * the device: a query that arrives while its algorithm's group runs joins a
+ * free source bit of it at the next iteration boundary, shares every later
+ * edge read of that traversal, and leaves with its result as soon as its own
+ * traversal is complete; the BFS and SSSP groups take turns.  An idle server
+ * runs a lone query on the single-source kernel.  With group_min =
+ * 0xFFFFFFFF, queries occupy slots of one resident traversal instead (u32
+ * values per slot, admitted the same way).  Results are bit-identical to
+ * thv_run of the same source. */
 typedef struct thv_server thv_server;
 
 typedef struct thv_serve_opts {
@@ -300,15 +305,18 @@ typedef struct thv_serve_opts {
   uint64_t mem_budget_bytes; /* device memory for per-query values (4 B per
                                 vertex per slot); 0 = all slots */
   uint32_t timeout_ms;       /* bound on device waits; 0 = 60000 */
-  uint32_t max_batch_iters;  /* iterations per launch while requests wait;
-                                0 = 4 */
-  uint32_t group_min;        /* batching: whenever the device is free, up
-                                to 64 waiting queries of the front query's
-                                algorithm run as one batched group (the
-                                thv_batch_run kernels) if at least group_min
-                                of them wait, else the front query runs
-                                alone; 0 = measured defaults (BFS 4, SSSP
-                                6); 0xFFFFFFFF = no batching (slots) */
+  uint32_t max_batch_iters;  /* slots: iterations per launch while requests
+                                wait; batched groups: iterations per launch
+                                while nothing waits and the other
+                                algorithm's group is idle (else 1); 0 = 4 */
+  uint32_t group_min;        /* batching: with nothing on the device, a
+                                batched group of an algorithm starts when
+                                at least group_min of its queries wait,
+                                else the front query runs alone; a running
+                                group admits every arrival of its algorithm
+                                it has room for; 0 = measured defaults (BFS
+                                4, SSSP 6); 0xFFFFFFFF = no batching
+                                (slots) */
   uint32_t replan_every;     /* re-place the graph's blocks by measured
                                 access (THV_PLACE_ACCESS, same budget) after
                                 this many finished queries; 0 = never */
@@ -323,8 +331,12 @@ typedef struct thv_query_stats {
   uint32_t slot;
   int32_t status;    /* thv_status of the query */
   uint32_t grouped;  /* 0: ran in a slot; 1: in a batched group (slot =
-                        position in it); 2: alone on the single-source
+                        its mask bit); 2: alone on the single-source
                         kernel (the server was idle) */
+  uint32_t joined;   /* 1: admitted into a group or slot traversal that was
+                        already running on the device (it joined mid-flight
+                        and shared that traversal's later iterations) */
+  uint32_t pad;
 } thv_query_stats;
 
 thv_status thv_serve_start(thv_graph *g, const thv_serve_opts *o,
@@ -362,8 +374,10 @@ thv_status thv_pick_sources(const thv_graph *g, uint64_t seed, uint32_t n,
  * (about 16 bytes per vertex plus 0.3 bytes per edge) get THV_ENOMEM.  Calls
  * share that array: calls whose work overlaps on the GPU race and must be
  * serialised by the caller.  The first call on a device looks up the
- * array's address; make it before any stream capture.  stream: a
- * cudaStream_t or NULL; iterations may be NULL.  Synchronous. */
+ * array's address; make it before any stream capture.  That address is kept
+ * for the life of the process: a cudaDeviceReset after the first call is not
+ * supported.  stream: a cudaStream_t or NULL; iterations may be NULL.
+ * Returns after the traversal has finished. */
 thv_status thv_bfs_noalloc(const uint64_t *d_off, const uint32_t *d_adj,
                            uint64_t nv, uint64_t ne, uint32_t source,
                            uint32_t *d_values, void *stream,

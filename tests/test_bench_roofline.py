@@ -2,6 +2,7 @@
 work-optimal run, split into HBM and host-link bytes, on hand-counted toy
 graphs (no GPU needed)."""
 import importlib.util
+import json
 import os
 
 import numpy as np
@@ -48,11 +49,26 @@ def test_whole_graph_algorithms_count_every_vertex_per_iteration(bench):
     assert edges == 5
 
 
-def test_captured_traffic_scales_with_edges(bench):
-    t = bench.NCU_TRAFFIC["sssp"]
-    dram, sysmem = bench.traffic_for("sssp", 24, 2 * t["ne"])
-    assert dram == 2 * t["dram"] and sysmem == 2 * t["sysmem"]
-    assert bench.traffic_for("no-such-kernel", 24, 1) == (None, None)
+def test_traffic_is_read_from_captures_of_the_same_workload(bench, tmp_path, monkeypatch):
+    table = tmp_path / "t.json"
+    table.write_text(json.dumps({"sssp_rmat24_wcsr_40%": {
+        "dram_read_bytes": 1000, "dram_write_bytes": 24, "sysmem_read_sectors": 10,
+        "command": "ncu ..."}}))
+    monkeypatch.setattr(bench, "TRAFFIC_TABLE", str(table))
+    dram, link, entry = bench.measured_traffic("sssp_rmat24_wcsr_40%")
+    assert dram == 1024 and link == 320 and entry["command"] == "ncu ..."
+    # a size that was not captured reports null, never a scaled guess
+    assert bench.measured_traffic("sssp_rmat26_wcsr_40%") == (None, None, None)
+    r = bench.roofline(100, 0, 1.0, 1.0, "measured", 1.0, 1.0, "sssp_rmat26_wcsr_40%", 1)
+    assert r["traffic"] is None and r["link_traffic"] is None
+
+
+def test_committed_traffic_table_entries_name_their_capture(bench):
+    if not os.path.exists(bench.TRAFFIC_TABLE):
+        pytest.skip("no captures committed")
+    for key, e in json.load(open(bench.TRAFFIC_TABLE)).items():
+        assert e["command"].startswith("ncu ") and "--clock-control none" in e["command"], key
+        assert e["dram_read_bytes"] > 0, key
 
 
 def test_union_find_bytes_skip_the_hub_component(bench):

@@ -162,3 +162,89 @@ def test_all_serving_modes_agree(T, O, g14w, eg, group_min):
             assert st["checksum"] == T.values_checksum(want(O, g14w, a, s)), (a, s)
         if group_min == 0xFFFFFFFF:
             assert 1 not in modes
+
+
+def graph_with_tail(O, T, tail, seed_scale=14):
+    """RMAT plus a path of `tail` vertices hanging off its highest-degree
+    vertex: traversals that reach the hub last about `tail` iterations, so a
+    batched group stays on the device long enough for arrivals to join."""
+    g = O.rmat(seed_scale, 16)
+    deg = np.diff(g.off.astype(np.int64))
+    hub = int(np.argmax(deg))
+    src = np.repeat(np.arange(g.nv, dtype=np.uint32), deg)
+    path = np.arange(g.nv, g.nv + tail, dtype=np.uint32)
+    s = np.concatenate([src, [hub], path[:-1]]).astype(np.uint32)
+    d = np.concatenate([g.adj, [g.nv], path[1:]]).astype(np.uint32)
+    gp = O.from_edges(g.nv + tail, s, d)
+    gp = O.CSR(gp.off, gp.adj, O.weights(gp))
+    eg = T.Graph.from_arrays(gp.off, gp.wcsr_edges(), "wcsr")
+    eg.plan(int(0.4 * eg.ne * 8), block_bytes=64 << 10)
+    return gp, eg, hub
+
+
+@pytest.mark.parametrize("algo,tail", [("sssp", 6000), ("bfs", 100)])
+def test_arrival_joins_a_running_batched_group(T, O, algo, tail):
+    # group_min 1: the first query starts a batched group at once; queries
+    # submitted while it runs must join it mid-flight (grouped 1, joined 1)
+    # with the answer of their solo run
+    gp, eg, hub = graph_with_tail(O, T, tail)
+    late = [int(x) for x in O.sources(gp, 40)][:4]
+    try:
+        with T.Server(eg, group_min=1, max_batch_iters=1, timeout_ms=20000) as sv:
+            first = sv.submit(algo, hub)
+            time.sleep(0.002)
+            tickets = []
+            for s in late:
+                tickets.append((sv.submit(algo, s), s))
+                time.sleep(0.0003)
+            vals, st = sv.wait(first)
+            assert st["grouped"] == 1 and st["joined"] == 0
+            assert np.array_equal(vals, want(O, gp, algo, hub))
+            joined = 0
+            for t, s in tickets:
+                vals, st = sv.wait(t)
+                w = want(O, gp, algo, s)
+                assert np.array_equal(vals, w), (algo, s)
+                assert st["checksum"] == T.values_checksum(w)
+                assert st["grouped"] == 1
+                joined += st["joined"]
+            assert joined >= 1, "no query joined the running group"
+    finally:
+        eg.close()
+
+
+def test_joined_sources_reuse_freed_bits(T, O):
+    # a long stream through one live group: more queries than mask bits, so
+    # bits of finished sources are reset and reused by later arrivals
+    gp, eg, hub = graph_with_tail(O, T, 120)
+    src = [int(x) for x in O.sources(gp, 150)]
+    try:
+        with T.Server(eg, group_min=1, timeout_ms=20000) as sv:
+            tickets = []
+            for i, s in enumerate(src):
+                tickets.append((sv.submit("bfs" if i % 3 else "sssp", s, want_values=(i % 7 == 0)), s, i))
+                if i % 10 == 0:
+                    time.sleep(0.001)
+            joined = 0
+            for t, s, i in tickets:
+                vals, st = sv.wait(t)
+                w = want(O, gp, "bfs" if i % 3 else "sssp", s)
+                assert st["checksum"] == T.values_checksum(w), (i, s)
+                if i % 7 == 0:
+                    assert np.array_equal(vals, w), (i, s)
+                joined += st["joined"]
+            assert joined > 0
+    finally:
+        eg.close()
+
+
+def test_group_deeper_than_the_level_bytes_falls_back_to_lone_runs(T, O):
+    # BFS levels past the u8 range: the group's queries run alone instead
+    gp, eg, hub = graph_with_tail(O, T, 300)
+    try:
+        with T.Server(eg, group_min=1, timeout_ms=20000) as sv:
+            vals, st = sv.wait(sv.submit("bfs", hub))
+            assert np.array_equal(vals, O.bfs(gp, hub))
+            assert st["grouped"] == 2
+    finally:
+        eg.close()

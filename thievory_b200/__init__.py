@@ -109,7 +109,8 @@ class _QueryStats(ctypes.Structure):
     _fields_ = [("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double),
                 ("latency_ms", ctypes.c_double), ("checksum", ctypes.c_uint64),
                 ("iterations", ctypes.c_uint32), ("slot", ctypes.c_uint32),
-                ("status", ctypes.c_int32), ("grouped", ctypes.c_uint32)]
+                ("status", ctypes.c_int32), ("grouped", ctypes.c_uint32),
+                ("joined", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
 
     def to_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}

@@ -58,6 +58,10 @@ struct MsCtrl {
   unsigned long long cnt_small[3], cnt_big[3], remaining[3], wc[3];
   unsigned minkept[3], pad;
   unsigned long long edges, hbm_bytes, link_bytes, pairs;
+  // live groups: where a launch that yielded stopped (the next launch
+  // resumes there), and the OR of the pending-source masks after it
+  unsigned y_iter, y_level, y_thr, y_width, yielded, pad2;
+  unsigned long long alive;
 };
 
 struct MsArgs {
@@ -83,6 +87,10 @@ struct MsArgs {
   uint32_t small_deg, chunk, delta;
   uint32_t wshift, wbase;  // packed weighted edges (see edge_dst / edge_wt)
   uint32_t growth;         // SSSP window width factor per advance
+  // live groups: a launch returns at the top of iteration yield_at (0 =
+  // run to completion); resume = 1 starts from r_* instead of iteration 0
+  uint32_t yield_at, resume;
+  uint32_t r_iter, r_level, r_thr, r_width;
 };
 
 struct BatchState {
@@ -445,7 +453,28 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
   uint32_t thr = OP == MS_SSSP ? (uint32_t)min(1ull + a.delta, 0xFFFFFFFFull) : 0xFFFFFFFFu;
   uint32_t width = a.delta;
   unsigned iter = 0, level = 1;  // BFS level of the vertices being expanded
+  if (a.resume) {
+    iter = a.r_iter;
+    level = a.r_level;
+    thr = a.r_thr;
+    width = a.r_width;
+  }
+  bool yielded = false;
   for (;; ++iter) {
+    // live groups return here, between iterations: every block has passed
+    // the previous iteration's last barrier, and the counter slot of this
+    // iteration was cleared during the previous one, so a later launch
+    // resumes exactly here
+    if (a.yield_at && iter >= a.yield_at) {
+      if (leader) {
+        c->y_iter = iter;
+        c->y_level = level;
+        c->y_thr = thr;
+        c->y_width = width;
+      }
+      yielded = true;
+      break;
+    }
     if (iter >= a.max_iters || (OP == MS_BFS && level > kMaxBfsLevel)) {
       if (leader) atomicCAS(&c->err, 0u, OP == MS_BFS && level > kMaxBfsLevel ? kDevErrDepth : kDevErrIters);
       break;
@@ -616,7 +645,10 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
     level++;
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
   }
-  if (leader) c->iters = iter;
+  if (leader) {
+    c->iters = iter;
+    c->yielded = yielded ? 1u : 0u;
+  }
 }
 
 template <int OP>
@@ -778,6 +810,164 @@ __global__ void __launch_bounds__(kExtractThreads) ms_checksum(MsArgs a, unsigne
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < k; i += blockDim.x)
     if (s_sum[i]) atomicAdd(sums + i, s_sum[i]);
+}
+
+// ------------------------------------------------------- live groups --
+// Continuous batching (the server): one group per algorithm stays on the
+// device between launches; arrivals take free mask bits and sources whose
+// pending set is empty retire, both between launches.  A source that joins
+// a running group keeps the single-source encoding relative to its start:
+//   BFS  its source vertex gets the group's current level byte L (the level
+//        expanded next), so its value at v is lvl[v][s] - (L - 1);
+//   SSSP its source vertex gets the current window's lower end b, so its
+//        value at v is dist[v][s] - (b - 1); its column starts at nv + b,
+//        the single-source "unreached" nv + 1 shifted the same way, so a
+//        relaxation stores only what the single-source run would store
+//        (distances below nv + 1).  The shared window then treats it as a
+//        source that started at distance b, the other sources' scale.
+// A group that has always started its sources at L = 1 / b = 1 is the
+// plain batched group.
+
+// OR of every vertex's pending-source mask: the sources still running.
+__global__ void ms_alive(const unsigned long long *front, uint32_t nv, unsigned long long *out) {
+  unsigned long long m = 0;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    m |= __ldcs(front + v);
+  m = warp_or(m);
+  if (lane_id() == 0 && m) atomicOr(out, m);
+}
+
+// Expands the low 4 bits of n into a byte mask (bit i -> byte i).
+__device__ __forceinline__ uint32_t byte_mask4(uint32_t n) {
+  return ((n & 1u) ? 0xFFu : 0u) | ((n & 2u) ? 0xFF00u : 0u) | ((n & 4u) ? 0xFF0000u : 0u) |
+         ((n & 8u) ? 0xFF000000u : 0u);
+}
+
+// Columns of the joining sources jm back to "unreached", 16 bytes of a row
+// per thread: BFS clears their visit bits and level bytes, SSSP writes each
+// source's shifted unreached value unreached[s].  Pending masks of these
+// bits are already empty (retired or never used).
+template <int OP>
+__global__ void ms_live_reset(MsArgs a, unsigned long long jm, const uint32_t *unreached) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (OP == MS_BFS) {
+    for (uint64_t v = tid; v < a.nv; v += stride) a.visit[v] &= ~jm;
+    uint4 *rows = reinterpret_cast<uint4 *>(a.lvl);
+    for (uint64_t i = tid; i < (uint64_t)a.nv * 4u; i += stride) {
+      const uint32_t q = (uint32_t)(i & 3u);  // bytes 16q .. 16q+15: sources 16q ..
+      const uint32_t bits = (uint32_t)(jm >> (16u * q)) & 0xFFFFu;
+      if (!bits) continue;
+      uint4 w = rows[i];
+      w.x &= ~byte_mask4(bits);
+      w.y &= ~byte_mask4(bits >> 4);
+      w.z &= ~byte_mask4(bits >> 8);
+      w.w &= ~byte_mask4(bits >> 12);
+      rows[i] = w;
+    }
+  } else {
+    uint4 *rows = reinterpret_cast<uint4 *>(a.dist);
+    for (uint64_t i = tid; i < (uint64_t)a.nv * 16u; i += stride) {
+      const uint32_t p = (uint32_t)(i & 15u);  // piece p: sources p, p+16, p+32, p+48
+      const uint32_t sel = (uint32_t)((jm >> p) & 1ull) | (uint32_t)((jm >> (p + 15u)) & 2ull) |
+                           (uint32_t)((jm >> (p + 30u)) & 4ull) | (uint32_t)((jm >> (p + 45u)) & 8ull);
+      if (!sel) continue;
+      uint4 w = rows[i];
+      if (sel & 1u) w.x = __ldg(unreached + p);
+      if (sel & 2u) w.y = __ldg(unreached + p + 16u);
+      if (sel & 4u) w.z = __ldg(unreached + p + 32u);
+      if (sel & 8u) w.w = __ldg(unreached + p + 48u);
+      rows[i] = w;
+    }
+  }
+}
+
+// k joining sources: bit bits[t] starts at vertex srcs[t] with value
+// vals[t] (BFS level byte, SSSP distance).
+template <int OP>
+__global__ void ms_live_seed(MsArgs a, uint32_t k, const uint32_t *bits, const uint32_t *srcs,
+                             const uint32_t *vals) {
+  const uint32_t t = threadIdx.x;
+  if (t >= k) return;
+  const uint32_t s = bits[t], v = srcs[t], val = vals[t];
+  atomicOr(a.front + v, 1ull << s);
+  atomicOr(a.bm + (v >> 5), 1u << (v & 31u));
+  if (OP == MS_BFS) {
+    atomicOr(a.visit + v, 1ull << s);
+    a.lvl[(size_t)v * kMsWidth + s] = (uint8_t)val;
+  } else {
+    a.dist[(size_t)v * kMsWidth + row_pos(s)] = val;
+    atomicMin(a.wmin + (v >> 5), val);
+  }
+}
+
+// Value of source s at a stored entry, in the single-source encoding, for a
+// source started at base b (BFS level byte / SSSP distance of its vertex).
+template <int OP>
+__device__ __forceinline__ uint32_t live_value(uint32_t raw, uint32_t b, uint32_t nv) {
+  if (OP == MS_BFS) return raw ? raw - (b - 1u) : nv + 1u;
+  return raw >= nv + b ? nv + 1u : raw - (b - 1u);
+}
+
+// Checksums of the finishing sources fin (rows read as they lie, only the
+// pieces holding a finishing source; see ms_checksum).
+template <int OP>
+__global__ void __launch_bounds__(kExtractThreads) ms_live_sums(MsArgs a, unsigned long long fin,
+                                                                const uint32_t *base,
+                                                                unsigned long long *sums) {
+  __shared__ unsigned long long s_sum[kMsWidth];
+  for (uint32_t i = threadIdx.x; i < kMsWidth; i += blockDim.x) s_sum[i] = 0;
+  __syncthreads();
+  const uint32_t l = threadIdx.x & 15u;
+  uint32_t src[4], b[4];
+  bool want[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    src[i] = OP == MS_BFS ? 4u * l + i : l + 16u * i;
+    want[i] = (fin >> src[i]) & 1ull;
+    b[i] = want[i] ? __ldg(base + src[i]) : 1u;
+  }
+  const bool any = want[0] || want[1] || want[2] || want[3];
+  unsigned long long acc[4] = {0, 0, 0, 0};
+  const uint64_t rows_per = kExtractThreads / 16;
+  for (uint64_t v = (uint64_t)blockIdx.x * rows_per + threadIdx.x / 16; any && v < a.nv;
+       v += (uint64_t)gridDim.x * rows_per) {
+    uint32_t raw[4];
+    if (OP == MS_BFS) {
+      const uint32_t w = __ldcs(reinterpret_cast<const uint32_t *>(a.lvl + v * kMsWidth) + l);
+#pragma unroll
+      for (int i = 0; i < 4; i++) raw[i] = (w >> (8 * i)) & 0xFFu;
+    } else {
+      const uint4 d = __ldcs(reinterpret_cast<const uint4 *>(a.dist + v * kMsWidth) + l);
+      raw[0] = d.x;
+      raw[1] = d.y;
+      raw[2] = d.z;
+      raw[3] = d.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (want[i]) acc[i] += value_hash((uint32_t)v, live_value<OP>(raw[i], b[i], a.nv));
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const unsigned long long t = acc[i] + __shfl_xor_sync(kFull, acc[i], 16);
+    if ((threadIdx.x & 31u) < 16u && t) atomicAdd(&s_sum[src[i]], t);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < kMsWidth; i += blockDim.x)
+    if (((fin >> i) & 1ull) && s_sum[i]) atomicAdd(sums + i, s_sum[i]);
+}
+
+// Values of one source (bit s, base b) into out[nv].
+template <int OP>
+__global__ void ms_live_column(MsArgs a, uint32_t s, uint32_t b, uint32_t *out) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < a.nv;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t raw = OP == MS_BFS ? (uint32_t)a.lvl[v * kMsWidth + s]
+                                      : a.dist[v * kMsWidth + row_pos(s)];
+    out[v] = live_value<OP>(raw, b, a.nv);
+  }
 }
 
 // ------------------------------------------------------------------ host --
@@ -1085,6 +1275,40 @@ static void tune_store(const std::string &key, const MsConfig &c) {
   fclose(f);
 }
 
+// Kernel arguments over batch state b (window, growth and tuning left at
+// their zero values for the caller to set).
+static MsArgs ms_args(thv_graph *g, BatchState *b, uint32_t timeout_ms) {
+  MsArgs a{};
+  a.off = g->d_off;
+  a.blk_vb = g->plan.d_vbegin;
+  a.blk_base = g->plan.d_base;
+  a.host_base = g->h_edges_dev;
+  a.lc = list_cache_of(g->plan);
+  a.blk_access = g->plan.d_access;
+  a.wshift = g->wshift;
+  a.wbase = g->wbase;
+  a.visit = b->d_visit;
+  a.front = b->d_front;
+  a.lvl = b->d_lvl;
+  a.dist = b->d_dist;
+  a.bm = b->d_bm;
+  a.wmin = b->d_wmin;
+  a.qs = b->d_qs;
+  a.qb = b->d_qb;
+  a.qsm = b->d_qsm;
+  a.qbm = b->d_qbm;
+  a.cap_s = b->cap_s;
+  a.cap_b = b->cap_b;
+  a.ctrl = b->d_ctrl;
+  a.sources = b->d_sources;
+  a.timeout_ns = (unsigned long long)timeout_ms * 1000000ull;
+  a.nblk = (uint32_t)g->plan.blocks.size();
+  a.nv = (uint32_t)g->nv;
+  a.ngroups = b->ngroups;
+  a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0x7FFFFFF0ull) * 2 + 8;
+  return a;
+}
+
 thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
                      uint32_t n, const thv_batch_opts *o, uint32_t *out,
                      uint64_t *checksums, thv_stats *stats) {
@@ -1117,35 +1341,8 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
   THV_TRY(ensure_batch_state(g, sssp, want_out));
   BatchState *b = g->bs;
   cudaStream_t st = o && o->stream ? (cudaStream_t)o->stream : g->stream;
-  MsArgs a{};
-  a.off = g->d_off;
-  a.blk_vb = g->plan.d_vbegin;
-  a.blk_base = g->plan.d_base;
-  a.host_base = g->h_edges_dev;
-  a.lc = list_cache_of(g->plan);
-  a.blk_access = g->plan.d_access;
-  a.wshift = g->wshift;
-  a.wbase = g->wbase;
-  a.visit = b->d_visit;
-  a.front = b->d_front;
-  a.lvl = b->d_lvl;
-  a.dist = b->d_dist;
-  a.bm = b->d_bm;
-  a.wmin = b->d_wmin;
-  a.qs = b->d_qs;
-  a.qb = b->d_qb;
-  a.qsm = b->d_qsm;
-  a.qbm = b->d_qbm;
-  a.cap_s = b->cap_s;
-  a.cap_b = b->cap_b;
-  a.ctrl = b->d_ctrl;
-  a.sources = b->d_sources;
   const uint32_t tmo = o && o->timeout_ms ? o->timeout_ms : 60000u;
-  a.timeout_ns = (unsigned long long)tmo * 1000000ull;
-  a.nblk = (uint32_t)g->plan.blocks.size();
-  a.nv = (uint32_t)g->nv;
-  a.ngroups = b->ngroups;
-  a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0x7FFFFFF0ull) * 2 + 8;
+  MsArgs a = ms_args(g, b, tmo);
   // Wide windows: many sources expand a vertex in the same iteration and
   // share its adjacency read (small windows make each source re-read it).
   // RMAT-26, 256 sources, weights 1..64: width 16 -> 36.6 q/s, 64 -> 74.8,
@@ -1230,6 +1427,222 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
   local.kernel_launches = launches;
   local.wall_ms = now_ms() - t0;
   if (stats) *stats = local;
+  return THV_OK;
+}
+
+// ------------------------------------------------------ live groups (host)
+
+// A joining BFS source needs this many levels of headroom below the u8
+// level range; an SSSP source needs its shifted values below 2^32.
+constexpr uint32_t kLiveBfsLevelRoom = 64;
+constexpr uint64_t kLiveSsspRoom = 1ull << 24;
+
+template <int OP, int ESZ, int THREADS>
+static thv_status live_launch(thv_graph *g, MsArgs &a, cudaStream_t st) {
+  BatchState *b = g->bs;
+  auto kern = ms_kernel<OP, ESZ, THREADS>;
+  const size_t ring = OP == MS_SSSP ? (size_t)THREADS / 32 * kMsRing * 512 : 0;
+  const size_t smem = ring + (g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0);
+  THV_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int bpsm = 0;
+  THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, THREADS, smem));
+  if (bpsm < 1) return fail(THV_ECUDA, "batch kernel cannot be resident");
+  unsigned long long *alive = reinterpret_cast<unsigned long long *>(
+      reinterpret_cast<char *>(b->d_ctrl) + offsetof(MsCtrl, alive));
+  THV_CUDA(cudaMemsetAsync(alive, 0, 8, st));
+  void *args[] = {&a};
+  THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(bpsm * g->num_sms), dim3(THREADS), args, smem, st));
+  ms_alive<<<g->num_sms * 4, 256, 0, st>>>(a.front, a.nv, alive);
+  THV_CUDA(cudaGetLastError());
+  THV_CUDA(cudaMemcpyAsync(b->h_ctrl, b->d_ctrl, sizeof(MsCtrl), cudaMemcpyDeviceToHost, st));
+  return THV_OK;
+}
+
+template <int OP>
+static thv_status live_launch_any(thv_graph *g, MsArgs &a, cudaStream_t st, uint32_t threads) {
+  if (g->esz == 8)
+    return threads == 256 ? live_launch<OP, 8, 256>(g, a, st) : live_launch<OP, 8, 512>(g, a, st);
+  return threads == 256 ? live_launch<OP, 4, 256>(g, a, st) : live_launch<OP, 4, 512>(g, a, st);
+}
+
+static MsArgs live_args(thv_graph *g, const LiveGroup *lg, uint32_t timeout_ms) {
+  MsArgs a = ms_args(g, g->bs, timeout_ms);
+  a.delta = kMsDelta;
+  a.growth = kMsGrowth;
+  a.small_deg = std::max(lg->small, kMsMinSmall);
+  a.chunk = std::max(lg->chunk, kMsMinChunk);
+  return a;
+}
+
+static thv_status live_state(thv_graph *g, const LiveGroup *lg) {
+  BatchState *b = g->bs_keep[lg->sssp ? 1 : 0];
+  if (!b || !b->valid) return fail(THV_EINVAL, "live group has no batch state");
+  g->bs = b;
+  return THV_OK;
+}
+
+thv_status live_open(thv_graph *g, LiveGroup *lg, bool sssp) {
+  lg->sssp = sssp;
+  lg->running = false;
+  lg->active = 0;
+  THV_TRY(dev_alloc((void **)&lg->d_buf, 4 * kMsWidth * 4, "live group staging"));
+  THV_TRY(pinned_alloc((void **)&lg->h_buf, 4 * kMsWidth * 4, "live group staging"));
+  THV_TRY(dev_alloc((void **)&lg->d_sums, kMsWidth * 8, "live group checksums"));
+  THV_TRY(pinned_alloc((void **)&lg->h_sums, kMsWidth * 8, "live group checksums"));
+  return ensure_batch_state(g, sssp, false);
+}
+
+void live_close(LiveGroup *lg) {
+  dev_free(lg->d_buf);
+  pinned_free(lg->h_buf);
+  dev_free(lg->d_sums);
+  pinned_free(lg->h_sums);
+  lg->d_buf = lg->h_buf = nullptr;
+  lg->d_sums = lg->h_sums = nullptr;
+  lg->running = false;
+  lg->active = 0;
+}
+
+bool live_can_join(const thv_graph *g, const LiveGroup *lg) {
+  if (!lg->running) return true;
+  if (__builtin_popcountll(lg->active) >= (int)kMsWidth) return false;
+  if (!lg->sssp) return lg->level + kLiveBfsLevelRoom <= kMaxBfsLevel;
+  return (uint64_t)lg->thr + g->nv + kLiveSsspRoom < 0xFFFFFFFFull;
+}
+
+thv_status live_add(thv_graph *g, LiveGroup *lg, uint32_t k, const uint32_t *sources,
+                    uint32_t *bits, uint32_t timeout_ms, cudaStream_t st) {
+  if (k == 0) return THV_OK;
+  if ((uint32_t)__builtin_popcountll(lg->active) + k > kMsWidth)
+    return fail(THV_EINVAL, "live group: %u sources do not fit", k);
+  const bool fresh = !lg->running;
+  if (fresh) {
+    THV_TRY(ensure_batch_state(g, lg->sssp, false));
+    MsConfig cfg = kMsDefault;
+    tune_lookup(tune_key(g, lg->sssp), &cfg);  // a configuration tuned by thv_batch_run
+    lg->small = cfg.small;
+    lg->chunk = cfg.chunk;
+    lg->threads = cfg.threads;
+    lg->iter = 0;
+    lg->level = 1;
+    lg->width = kMsDelta;
+    lg->thr = (uint32_t)std::min<uint64_t>(1ull + kMsDelta, 0xFFFFFFFFull);
+    lg->active = 0;
+  }
+  THV_TRY(live_state(g, lg));
+  BatchState *b = g->bs;
+  MsArgs a = live_args(g, lg, timeout_ms);
+  // value of the joining sources' vertices: BFS the level expanded next,
+  // SSSP the lower end of the current window
+  const uint32_t start = lg->sssp ? (uint32_t)std::max<int64_t>(1, (int64_t)lg->thr - lg->width)
+                                  : lg->level;
+  uint32_t *hb = lg->h_buf;  // [bits | sources | seed values | unreached per bit]
+  unsigned long long jm = 0;
+  uint32_t t = 0;
+  for (uint32_t s = 0; s < kMsWidth && t < k; s++) {
+    if ((lg->active >> s) & 1ull) continue;
+    hb[t] = s;
+    hb[kMsWidth + t] = sources[t];
+    hb[2 * kMsWidth + t] = start;
+    bits[t] = s;
+    jm |= 1ull << s;
+    lg->base[s] = start;
+    t++;
+  }
+  for (uint32_t s = 0; s < kMsWidth; s++)
+    hb[3 * kMsWidth + s] = (uint32_t)(g->nv + ((jm >> s) & 1ull ? start : 1u));
+  THV_CUDA(cudaMemcpyAsync(lg->d_buf, hb, 4 * kMsWidth * 4, cudaMemcpyHostToDevice, st));
+  const int igrid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 255) / 256)));
+  if (fresh) {
+    if (lg->sssp) ms_init<MS_SSSP><<<igrid, 256, 0, st>>>(a, b->ngroups * 32u);
+    else ms_init<MS_BFS><<<igrid, 256, 0, st>>>(a, b->ngroups * 32u);
+  } else {
+    if (lg->sssp) ms_live_reset<MS_SSSP><<<igrid, 256, 0, st>>>(a, jm, lg->d_buf + 3 * kMsWidth);
+    else ms_live_reset<MS_BFS><<<igrid, 256, 0, st>>>(a, jm, lg->d_buf + 3 * kMsWidth);
+  }
+  if (lg->sssp)
+    ms_live_seed<MS_SSSP><<<1, kMsWidth, 0, st>>>(a, k, lg->d_buf, lg->d_buf + kMsWidth, lg->d_buf + 2 * kMsWidth);
+  else
+    ms_live_seed<MS_BFS><<<1, kMsWidth, 0, st>>>(a, k, lg->d_buf, lg->d_buf + kMsWidth, lg->d_buf + 2 * kMsWidth);
+  THV_CUDA(cudaGetLastError());
+  THV_CUDA(cudaStreamSynchronize(st));
+  lg->active |= jm;
+  lg->running = true;
+  return THV_OK;
+}
+
+thv_status live_step(thv_graph *g, LiveGroup *lg, uint32_t iters, uint32_t timeout_ms,
+                     cudaStream_t st, unsigned long long *finished, bool *too_deep) {
+  *finished = 0;
+  *too_deep = false;
+  if (!lg->running || !lg->active) return THV_OK;
+  THV_TRY(live_state(g, lg));
+  BatchState *b = g->bs;
+  MsArgs a = live_args(g, lg, timeout_ms);
+  a.resume = 1;
+  a.r_iter = lg->iter;
+  a.r_level = lg->level;
+  a.r_thr = lg->thr;
+  a.r_width = lg->width;
+  a.yield_at = lg->iter + std::max(iters, 1u);
+  a.max_iters = 0xFFFFFFF0u;
+  THV_TRY(lg->sssp ? live_launch_any<MS_SSSP>(g, a, st, lg->threads)
+                   : live_launch_any<MS_BFS>(g, a, st, lg->threads));
+  THV_CUDA(cudaStreamSynchronize(st));
+  const MsCtrl &hc = *b->h_ctrl;
+  if (hc.err == kDevErrDepth) {
+    *too_deep = true;
+    return THV_OK;
+  }
+  if (hc.err == kDevErrBarrier) return fail(THV_ETIMEOUT, "grid barrier wait exceeded %u ms", timeout_ms);
+  if (hc.err == kDevErrIters) return fail(THV_ETIMEOUT, "iteration cap reached");
+  if (hc.err) return fail(THV_EDEVICE, "batch device error %u", hc.err);
+  lg->edges = hc.edges;
+  lg->hbm_bytes = hc.hbm_bytes;
+  lg->link_bytes = hc.link_bytes;
+  if (hc.yielded) {
+    lg->iter = hc.y_iter;
+    lg->level = hc.y_level;
+    lg->thr = hc.y_thr;
+    lg->width = hc.y_width;
+    *finished = lg->active & ~hc.alive;
+  } else {
+    lg->iter = hc.iters;
+    *finished = lg->active;  // no pending pair left: every source is done
+  }
+  return THV_OK;
+}
+
+thv_status live_collect(thv_graph *g, LiveGroup *lg, unsigned long long fin, uint64_t *sums,
+                        uint32_t *const *out, uint32_t *d_stage, cudaStream_t st) {
+  fin &= lg->active;
+  if (!fin) return THV_OK;
+  THV_TRY(live_state(g, lg));
+  MsArgs a = live_args(g, lg, 60000u);
+  uint32_t *hb = lg->h_buf + 3 * kMsWidth;
+  for (uint32_t s = 0; s < kMsWidth; s++) hb[s] = (fin >> s) & 1ull ? lg->base[s] : 1u;
+  THV_CUDA(cudaMemcpyAsync(lg->d_buf + 3 * kMsWidth, hb, kMsWidth * 4, cudaMemcpyHostToDevice, st));
+  THV_CUDA(cudaMemsetAsync(lg->d_sums, 0, kMsWidth * 8, st));
+  if (lg->sssp)
+    ms_live_sums<MS_SSSP><<<g->num_sms * 8, kExtractThreads, 0, st>>>(a, fin, lg->d_buf + 3 * kMsWidth, lg->d_sums);
+  else
+    ms_live_sums<MS_BFS><<<g->num_sms * 8, kExtractThreads, 0, st>>>(a, fin, lg->d_buf + 3 * kMsWidth, lg->d_sums);
+  THV_CUDA(cudaGetLastError());
+  THV_CUDA(cudaMemcpyAsync(lg->h_sums, lg->d_sums, kMsWidth * 8, cudaMemcpyDeviceToHost, st));
+  const int grid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 255) / 256)));
+  for (uint32_t s = 0; s < kMsWidth; s++) {
+    if (!((fin >> s) & 1ull) || !out || !out[s]) continue;
+    if (lg->sssp) ms_live_column<MS_SSSP><<<grid, 256, 0, st>>>(a, s, lg->base[s], d_stage);
+    else ms_live_column<MS_BFS><<<grid, 256, 0, st>>>(a, s, lg->base[s], d_stage);
+    THV_CUDA(cudaGetLastError());
+    THV_CUDA(cudaMemcpyAsync(out[s], d_stage, g->nv * 4, cudaMemcpyDeviceToHost, st));
+    THV_CUDA(cudaStreamSynchronize(st));  // d_stage is reused by the next source
+  }
+  THV_CUDA(cudaStreamSynchronize(st));
+  for (uint32_t s = 0; s < kMsWidth; s++)
+    if ((fin >> s) & 1ull) sums[s] = lg->h_sums[s];
+  lg->active &= ~fin;
+  if (!lg->active) lg->running = false;
   return THV_OK;
 }
 

@@ -19,6 +19,14 @@
 // column, admits waiting requests into free slots (seeding their sources)
 // and relaunches: a request that arrives while others run joins at the next
 // launch boundary and shares every later edge read with them.
+//
+// The default mode runs the same admission on the batched kernels instead
+// (batch.cu, live groups): one group per algorithm with 64-bit source
+// masks (BFS levels in bytes, SSSP distances in 64-wide rows), each launch
+// running one iteration or a few, finished sources retiring and waiting
+// queries joining free mask bits between launches; the BFS and SSSP groups
+// take turns on the device.  An idle server runs a lone query on the
+// single-source kernel, which is faster for one query than a group.
 #include <algorithm>
 #include <chrono>
 #include <cstddef>
@@ -70,12 +78,6 @@ struct SvArgs {
   uint32_t wshift, wbase;  // 4-byte edges: see edge_dst / edge_wt
   uint32_t pad;
 };
-
-__device__ __forceinline__ unsigned long long warp_or(unsigned long long x) {
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) x |= __shfl_xor_sync(kFull, x, d);
-  return x;
-}
 
 __device__ __forceinline__ void sv_edge(const SvArgs &a, uint32_t u, uint32_t w, uint32_t wt,
                                         unsigned long long f) {
@@ -476,6 +478,7 @@ struct Query {
   thv_status status = THV_OK;
   bool done = false;
   uint32_t mode = 0;  // 0 slot, 1 batched group, 2 single-source run
+  bool joined = false;  // admitted into a batched group that was already running
 };
 
 // Batched-group mode: device bytes per vertex of the batch state (masks,
@@ -521,6 +524,12 @@ struct thv_server {
   thv_status fatal = THV_OK;
   std::string fatal_msg;
   std::thread worker;
+  // batching: one live group per algorithm (BFS, SSSP) and the ticket and
+  // start iteration of each mask bit
+  LiveGroup live[2];
+  bool live_open[2] = {false, false};
+  uint64_t live_ticket[2][64] = {};
+  uint32_t live_iter0[2][64] = {};
 };
 
 namespace {
@@ -531,6 +540,8 @@ double clock_ms() {
 }
 
 void server_free(thv_server *s) {
+  for (int k = 0; k < 2; k++)
+    if (s->live_open[k]) live_close(&s->live[k]);
   dev_free(s->d_val);
   dev_free(s->d_bm);
   dev_free(s->d_out);
@@ -661,41 +672,84 @@ void fail_all(thv_server *s, thv_status st, const std::string &msg) {
   s->cv_done.notify_all();
 }
 
-// Runs waiting queries of one algorithm as a batched group (one shared
-// traversal per up-to-64 sources), writing each query's values and checksum.
-thv_status run_grouped(thv_server *s, thv_algo algo, const std::vector<uint64_t> &tickets) {
-  const uint32_t n = (uint32_t)tickets.size();
-  std::vector<uint32_t> src(n);
-  std::vector<uint32_t *> rows(n);
-  std::vector<uint64_t> sums(n, 0);
+// Iterations per launch of a live group: one while anything waits to join
+// or the other algorithm's group shares the device (so admission and the
+// turns stay short), else thv_serve_opts.max_batch_iters (default 4: fewer
+// returns to the host).
+constexpr uint32_t kLiveItersBusy = 1;
+
+// Adds tickets (all of algorithm k) to live group k, opening it on first use.
+thv_status live_join(thv_server *s, int k, const std::vector<uint64_t> &tickets) {
+  if (tickets.empty()) return THV_OK;
+  thv_graph *g = s->g;
+  if (!s->live_open[k]) {
+    THV_TRY(live_open(g, &s->live[k], k == 1));
+    s->live_open[k] = true;
+  }
+  std::vector<uint32_t> src(tickets.size()), bits(tickets.size());
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    for (uint32_t i = 0; i < n; i++) {
-      const Query &q = s->queries[tickets[i]];
-      src[i] = q.source;
-      rows[i] = q.out;
+    for (size_t i = 0; i < tickets.size(); i++) src[i] = s->queries[tickets[i]].source;
+  }
+  THV_TRY(live_add(g, &s->live[k], (uint32_t)src.size(), src.data(), bits.data(),
+                   (uint32_t)(s->timeout_ns / 1000000ull), s->st));
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (size_t i = 0; i < tickets.size(); i++) {
+    s->live_ticket[k][bits[i]] = tickets[i];
+    s->live_iter0[k][bits[i]] = s->live[k].iter;
+    s->queries[tickets[i]].slot = bits[i];
+  }
+  return THV_OK;
+}
+
+thv_status run_alone(thv_server *s, thv_algo algo, uint64_t ticket);
+
+// One launch of live group k, then its finished sources' results.
+thv_status live_turn(thv_server *s, int k, uint32_t iters) {
+  LiveGroup &lg = s->live[k];
+  unsigned long long fin = 0;
+  bool too_deep = false;
+  const uint32_t tmo = (uint32_t)(s->timeout_ns / 1000000ull);
+  THV_TRY(live_step(s->g, &lg, iters, tmo, s->st, &fin, &too_deep));
+  if (too_deep) {
+    // a BFS level left the u8 range: its queries run alone instead
+    std::vector<uint64_t> redo;
+    for (unsigned long long m = lg.active; m; m &= m - 1) redo.push_back(s->live_ticket[k][__builtin_ctzll(m)]);
+    lg.active = 0;
+    lg.running = false;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      for (uint64_t t : redo) s->queries[t].mode = 2;
+    }
+    for (uint64_t t : redo) THV_TRY(run_alone(s, k ? THV_ALGO_SSSP : THV_ALGO_BFS, t));
+    return THV_OK;
+  }
+  if (!fin) return THV_OK;
+  uint32_t *outs[64] = {};
+  uint64_t sums[64] = {};
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (unsigned long long m = fin; m; m &= m - 1) {
+      const int b = __builtin_ctzll(m);
+      outs[b] = s->queries[s->live_ticket[k][b]].out;
     }
   }
-  thv_batch_opts bo{};
-  bo.timeout_ms = (uint32_t)(s->timeout_ns / 1000000ull);
-  bo.stream = s->st;  // a configuration tuned by an earlier thv_batch_run is reused
-  thv_stats bst{};
-  const thv_status st = run_batch_rows(s->g, algo, src.data(), n, &bo, rows.data(), sums.data(), &bst);
+  THV_TRY(live_collect(s->g, &lg, fin, sums, outs, s->d_out, s->st));
   std::lock_guard<std::mutex> lk(s->mu);
   const double now = clock_ms();
-  for (uint32_t i = 0; i < n; i++) {
-    Query &q = s->queries[tickets[i]];
-    q.checksum = sums[i];
+  for (unsigned long long m = fin; m; m &= m - 1) {
+    const int b = __builtin_ctzll(m);
+    Query &q = s->queries[s->live_ticket[k][b]];
+    q.checksum = sums[b];
     q.t_done = now;
-    q.iterations = (uint32_t)bst.iterations;
-    q.slot = i;
-    q.status = st;
+    q.iterations = lg.iter - s->live_iter0[k][b];
+    q.status = THV_OK;
     q.done = true;
+    s->live_ticket[k][b] = 0;
+    s->done_since_replan++;
   }
-  s->total_iters += bst.iterations;
-  s->done_since_replan += n;
   s->cv_done.notify_all();
-  return st;
+  return THV_OK;
 }
 
 // One query on the single-source kernel (values into its buffer, checksum).
@@ -729,22 +783,92 @@ thv_status run_alone(thv_server *s, thv_algo algo, uint64_t ticket) {
   return st;
 }
 
+bool live_running(const thv_server *s) { return s->live[0].running || s->live[1].running; }
+
+// Batching mode, one dispatcher round: admit waiting queries into the live
+// groups (a running group takes them into free mask bits; a group that is
+// not running starts when enough of its algorithm wait, or at once when the
+// other algorithm's group is on the device), run a lone query when nothing
+// is live and too few wait, then give each running group one turn.
+thv_status batching_round(thv_server *s) {
+  std::vector<uint64_t> joins[2];
+  uint64_t alone = 0;
+  thv_algo alone_algo = THV_ALGO_BFS;
+  bool waiting_for[2] = {false, false};
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    const double now = clock_ms();
+    for (int k = 0; k < 2; k++) {
+      const thv_algo algo = k ? THV_ALGO_SSSP : THV_ALGO_BFS;
+      uint32_t n = 0;
+      for (uint64_t t : s->waiting) n += s->queries[t].algo == algo;
+      if (!n) continue;
+      LiveGroup &lg = s->live[k];
+      const bool running = lg.running;
+      uint32_t take = 0;
+      if (running) {
+        if (live_can_join(s->g, &lg)) take = std::min<uint32_t>(n, kGroupMax - __builtin_popcountll(lg.active));
+      } else {
+        const uint32_t kmin = s->group_min ? s->group_min : (k ? kGroupMinSssp : kGroupMinBfs);
+        if (n >= kmin || s->live[1 - k].running) take = std::min<uint32_t>(n, kGroupMax);
+      }
+      waiting_for[k] = take < n;
+      for (auto it = s->waiting.begin(); it != s->waiting.end() && joins[k].size() < take;) {
+        Query &q = s->queries[*it];
+        if (q.algo != algo) {
+          ++it;
+          continue;
+        }
+        q.t_start = now;
+        q.mode = 1;
+        q.joined = running;
+        joins[k].push_back(*it);
+        it = s->waiting.erase(it);
+      }
+    }
+    if (joins[0].empty() && joins[1].empty() && !live_running(s) && !s->waiting.empty()) {
+      alone = s->waiting.front();
+      s->waiting.pop_front();
+      Query &q = s->queries[alone];
+      q.t_start = clock_ms();
+      q.mode = 2;
+      alone_algo = q.algo;
+    }
+  }
+  if (alone) return run_alone(s, alone_algo, alone);
+  for (int k = 0; k < 2; k++) THV_TRY(live_join(s, k, joins[k]));
+  const bool both = s->live[0].running && s->live[1].running;
+  for (int k = 0; k < 2; k++) {
+    if (!s->live[k].running) continue;
+    bool waits;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      waits = !s->waiting.empty();
+    }
+    const uint32_t iters = both || waits || waiting_for[k] ? kLiveItersBusy : s->batch_iters;
+    THV_TRY(live_turn(s, k, iters));
+  }
+  return THV_OK;
+}
+
 void worker_loop(thv_server *s) {
   cudaSetDevice(s->g->device);
   for (;;) {
     uint32_t nseed = 0;
     bool requests_waiting = false;
-    std::vector<uint64_t> group;
-    thv_algo galgo = THV_ALGO_BFS;
+    uint64_t lone = 0;
+    thv_algo lone_algo = THV_ALGO_BFS;
     bool replan = false;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_work.wait(lk, [&] { return s->stopping || !s->waiting.empty() || s->active; });
-      if (s->stopping && s->waiting.empty() && !s->active) return;
-      // between queries (no slot running), re-place the edge blocks by the
-      // access this server measured
-      if (s->replan_every && !s->active && s->done_since_replan >= s->replan_every &&
-          (s->g->plan.flags & THV_PLAN_TRACK_ACCESS)) {
+      s->cv_work.wait(lk, [&] {
+        return s->stopping || !s->waiting.empty() || s->active || live_running(s);
+      });
+      if (s->stopping && s->waiting.empty() && !s->active && !live_running(s)) return;
+      // between queries (nothing on the device), re-place the edge blocks by
+      // the access this server measured
+      if (s->replan_every && !s->active && !live_running(s) &&
+          s->done_since_replan >= s->replan_every && (s->g->plan.flags & THV_PLAN_TRACK_ACCESS)) {
         s->done_since_replan = 0;
         replan = true;
       }
@@ -757,56 +881,28 @@ void worker_loop(thv_server *s) {
       }
       continue;
     }
+    if (s->batching) {
+      const thv_status st = batching_round(s);
+      if (st != THV_OK) {
+        fail_all(s, st, thv_last_error());
+        return;
+      }
+      continue;
+    }
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      // A deep queue runs as batched groups: stop admitting into slots, and
-      // once the slots have drained take up to 64 waiting queries of the
-      // front query's algorithm (FIFO within that algorithm).
-      // Batching: whenever the device is free, the front query's algorithm
-      // runs as one batched group of up to 64 waiting queries if enough of
-      // them wait, else the front query runs alone on the single-source
-      // kernel.  Without batching: lone runs when one query waits, slots
-      // (admission into the running traversal) otherwise.
-      const bool deep = s->batching;
-      if (s->batching && !s->active && !s->waiting.empty()) {
-        galgo = s->queries[s->waiting.front()].algo;
-        uint32_t k = 0;
-        for (uint64_t t : s->waiting) k += s->queries[t].algo == galgo;
-        const uint32_t kmin = s->group_min ? s->group_min
-                                           : (galgo == THV_ALGO_BFS ? kGroupMinBfs : kGroupMinSssp);
-        if (k >= kmin) {
-          for (auto it = s->waiting.begin(); it != s->waiting.end() && group.size() < kGroupMax;) {
-            if (s->queries[*it].algo == galgo) {
-              group.push_back(*it);
-              it = s->waiting.erase(it);
-            } else {
-              ++it;
-            }
-          }
-          const double now = clock_ms();
-          for (uint64_t t : group) {
-            Query &q = s->queries[t];
-            q.t_start = now;
-            q.mode = 1;
-          }
-        } else {
-          group.push_back(s->waiting.front());
-          s->waiting.pop_front();
-          Query &q = s->queries[group[0]];
-          q.t_start = clock_ms();
-          q.mode = 2;
-        }
-      } else if (!s->batching && !s->active && s->waiting.size() == 1) {
-        // an idle server with one request: the single-source kernel
-        group.push_back(s->waiting.front());
+      // Slots: an idle server with one request runs it on the single-source
+      // kernel; otherwise each waiting query takes a free slot (its column
+      // was reset when the slot's last query retired).
+      if (!s->active && s->waiting.size() == 1) {
+        lone = s->waiting.front();
         s->waiting.pop_front();
-        Query &q = s->queries[group[0]];
-        galgo = q.algo;
+        Query &q = s->queries[lone];
+        lone_algo = q.algo;
         q.t_start = clock_ms();
         q.mode = 2;
       }
-      // admission: free slot (its column is reset) for each waiting query
-      while (!deep && !s->waiting.empty()) {
+      while (!lone && !s->waiting.empty()) {
         int slot = -1;
         for (uint32_t i = 0; i < s->W; i++)
           if (!((s->active >> i) & 1ull)) { slot = (int)i; break; }
@@ -817,6 +913,7 @@ void worker_loop(thv_server *s) {
         q.slot = (uint32_t)slot;
         q.t_start = clock_ms();
         q.iter_start = (uint32_t)s->total_iters;
+        q.joined = s->active != 0;
         const bool bfs = q.algo == THV_ALGO_BFS;
         s->h_seeds[nseed++] = SvSeed{(uint32_t)slot, q.source, bfs ? 2u : 1u + kSvDeltaSssp,
                                      bfs ? 1u : kSvDeltaSssp};
@@ -827,12 +924,10 @@ void worker_loop(thv_server *s) {
       // with a free slot, return to the host every few iterations so that a
       // request arriving meanwhile is admitted quickly; with none free, run
       // until a query finishes
-      requests_waiting = !deep && __builtin_popcountll(s->active) < (int)s->W;
+      requests_waiting = __builtin_popcountll(s->active) < (int)s->W;
     }
-    if (!group.empty()) {
-      const thv_status st = group.size() == 1 && s->queries[group[0]].mode == 2
-                                ? run_alone(s, galgo, group[0])
-                                : run_grouped(s, galgo, group);
+    if (lone) {
+      const thv_status st = run_alone(s, lone_algo, lone);
       if (st != THV_OK) {
         fail_all(s, st, thv_last_error());
         return;
@@ -889,6 +984,15 @@ thv_status start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
   if (o && o->mem_budget_bytes && o->mem_budget_bytes < g->nv * kGroupBytesPerVertex)
     s->batching = false;  // the batch state does not fit the memory budget
   s->timeout_ns = (uint64_t)(o && o->timeout_ms ? o->timeout_ms : 60000u) * 1000000ull;
+  THV_TRY(dev_alloc((void **)&s->d_out, g->nv * 4 + 64, "serving output"));
+  THV_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  if (s->batching) {
+    // live groups allocate their batch state on first use
+    thv_server *raw = s.release();
+    raw->worker = std::thread(worker_loop, raw);
+    *out = raw;
+    return THV_OK;
+  }
   const uint64_t nw = (g->nv + 31) / 32;
   s->ngroups = (uint32_t)((nw + 31) / 32);
   const uint64_t nw_alloc = (uint64_t)s->ngroups * 32;
@@ -897,7 +1001,6 @@ thv_status start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
   THV_TRY(dev_alloc((void **)&s->d_val, g->nv * (uint64_t)W * 4 + 64, "serving values"));
   THV_TRY(dev_alloc((void **)&s->d_front, g->nv * 8 + 64, "serving masks"));
   THV_TRY(dev_alloc((void **)&s->d_bm, nw_alloc * 4, "serving bitmap"));
-  THV_TRY(dev_alloc((void **)&s->d_out, g->nv * 4 + 64, "serving output"));
   THV_TRY(dev_alloc((void **)&s->d_qs, s->cap_s * sizeof(WorkItem), "serving queue"));
   THV_TRY(dev_alloc((void **)&s->d_qsm, s->cap_s * 8, "serving queue masks"));
   THV_TRY(dev_alloc((void **)&s->d_qb, s->cap_b * sizeof(WorkItem), "serving chunk queue"));
@@ -908,7 +1011,6 @@ thv_status start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
   THV_TRY(pinned_alloc((void **)&s->h_seeds, kSvMaxSlots * sizeof(SvSeed), "serving seeds"));
   THV_TRY(dev_alloc((void **)&s->d_sum, 8, "serving checksum"));
   THV_TRY(pinned_alloc((void **)&s->h_sum, 8, "serving checksum"));
-  THV_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   SvArgs a = make_args(s.get());
   const int grid = std::max(1, std::min<int>(g->num_sms * 8, (int)((g->nv + 255) / 256)));
   sv_reset<<<grid, 256, 0, s->st>>>(a, (uint32_t)nw_alloc);
@@ -972,6 +1074,8 @@ static thv_status collect(thv_server *s, uint64_t ticket, thv_query_stats *st) {
     st->slot = q.slot;
     st->status = q.status;
     st->grouped = q.mode;
+    st->joined = q.joined ? 1u : 0u;
+    st->pad = 0;
   }
   const thv_status qs = q.status;
   s->queries.erase(it);

@@ -69,6 +69,12 @@ __device__ __forceinline__ T warp_sum(T x) {
   return x;
 }
 
+__device__ __forceinline__ unsigned long long warp_or(unsigned long long x) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) x |= __shfl_xor_sync(kFull, x, d);
+  return x;
+}
+
 __device__ __forceinline__ unsigned warp_min(unsigned x) {
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) x = min(x, __shfl_xor_sync(kFull, x, d));

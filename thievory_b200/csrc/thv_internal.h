@@ -196,6 +196,39 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
                           uint64_t *checksums, thv_stats *stats);
 void batch_free(thv_graph *g);
 
+// Continuous batched group of the server (batch.cu): up to 64 sources of
+// one algorithm share a traversal that stays on the device; between
+// launches, sources whose pending set is empty retire (live_collect) and
+// new ones join free mask bits (live_add), each keeping its single-source
+// encoding relative to its own start (base).
+struct LiveGroup {
+  bool sssp = false, running = false;
+  uint32_t small = 64, chunk = 256, threads = 512;  // launch configuration
+  uint32_t iter = 0, level = 1, thr = 0, width = 0;  // where the next launch resumes
+  unsigned long long active = 0;                     // mask bits in use
+  uint32_t base[64] = {};  // per bit: BFS level byte / SSSP distance of its source vertex
+  uint32_t *d_buf = nullptr, *h_buf = nullptr;       // 4 x 64 u32 staging
+  unsigned long long *d_sums = nullptr, *h_sums = nullptr;
+  uint64_t edges = 0, hbm_bytes = 0, link_bytes = 0;  // since the group started
+};
+thv_status live_open(thv_graph *g, LiveGroup *lg, bool sssp);
+void live_close(LiveGroup *lg);
+// Whether a running group can take another source (free bit, BFS level and
+// SSSP distance headroom); a group that is not running always can.
+bool live_can_join(const thv_graph *g, const LiveGroup *lg);
+// Adds k sources (a fresh traversal if the group is not running); bits[t]
+// receives the mask bit of sources[t].
+thv_status live_add(thv_graph *g, LiveGroup *lg, uint32_t k, const uint32_t *sources,
+                    uint32_t *bits, uint32_t timeout_ms, cudaStream_t st);
+// Runs up to `iters` iterations; *finished = bits whose sources are done;
+// *too_deep when a BFS level left the u8 range (the group must be dropped).
+thv_status live_step(thv_graph *g, LiveGroup *lg, uint32_t iters, uint32_t timeout_ms,
+                     cudaStream_t st, unsigned long long *finished, bool *too_deep);
+// Checksums (sums[bit]) and, where out[bit] is set, values of the finished
+// bits (via the device buffer d_stage of nv u32); frees the bits.
+thv_status live_collect(thv_graph *g, LiveGroup *lg, unsigned long long fin, uint64_t *sums,
+                        uint32_t *const *out, uint32_t *d_stage, cudaStream_t st);
+
 thv_status generate_rmat(const thv_rmat_opts *o, thv_format fmt, int device,
                          thv_graph **out);
 
