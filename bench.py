@@ -100,11 +100,20 @@ def parse(argv=None):
                     help="c4: batched sources (default 1024); c5: queries per rate (default 96)")
     ap.add_argument("--group-min", type=int, default=0,
                     help="c5: queue depth from which the server runs batched groups (0 = default)")
+    ap.add_argument("--join-window", type=int, default=0,
+                    help="c5: iterations a running group admits arrivals (0 = the server's "
+                         "default, 0xFFFFFFFF = its whole life)")
+    ap.add_argument("--groups-per-algo", type=int, default=0,
+                    help="c5: batched groups of one algorithm on the device at once (0 = default)")
     ap.add_argument("--scale", type=int, default=0, help="override the workload's scale")
     ap.add_argument("--source", type=int, default=1, help="BFS/SSSP source vertex")
     ap.add_argument("--budget-frac", type=float, default=-1.0,
                     help="override the HBM edge budget as a fraction of edge bytes")
     ap.add_argument("--no-extra", action="store_true", help="headline workload only")
+    ap.add_argument("--edge-packing", type=int, default=1, choices=[0, 1],
+                    help="weighted graphs: 4-byte packed edges (1) or 8-byte {dst, w} (0)")
+    ap.add_argument("--label-propagation", action="store_true",
+                    help="c2cc: min-label propagation instead of union-find")
     ap.add_argument("--only", default="", help="comma-separated extra sections to run")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--time-guard-s", type=float, default=600.0,
@@ -125,6 +134,17 @@ def budget_desc(wl):
     if "budget" in wl:
         return f"{wl['budget']} bytes"
     return f"{int(round(wl['frac'] * 100))}% of the format's edge bytes"
+
+
+def traffic_key(wl, packed=True, label_propagation=False):
+    """Name of a workload in the traffic table: algorithm (CC: method),
+    scale, format, budget, edge storage."""
+    algo = wl["algo"]
+    if algo == "cc":
+        algo = "cc_lp" if label_propagation or not wl["sym"] else "cc_uf"
+    budget = f"{wl['budget'] >> 20}MiB" if "budget" in wl else f"{int(round(wl['frac'] * 100))}pct"
+    return f"{algo}_rmat{wl['scale']}_{wl['fmt']}{'_sym' if wl['sym'] else ''}_{budget}" + \
+        ("" if packed or wl["fmt"] != "wcsr" else "_unpacked")
 
 
 def workload_config(wl, source, gpus):
@@ -477,10 +497,17 @@ def run_headline(b, args):
     if args.budget_frac >= 0:
         wl.pop("budget", None)
         wl["frac"] = args.budget_frac
-    key = f"{wl['algo']}_rmat{wl['scale']}_{wl['fmt']}_{budget_desc(wl).split()[0]}"
+    key = traffic_key(wl, packed=bool(args.edge_packing), label_propagation=args.label_propagation)
     keep = args.workload == "c2" and not args.no_extra and b.dist.world == 1
+    graph = None
+    if not args.edge_packing:
+        graph = b.gen(wl)
+        graph.set_edge_packing(False)
+    run_kw = {"label_propagation": True} if args.label_propagation else None
     main = b.measure(wl, args.steps, args.warmup, want_e2e=True, cpu=not args.no_cpu,
-                     traffic_key=key, keep=keep)
+                     traffic_key=key, keep=keep, graph=graph, run_kw=run_kw)
+    if graph is not None and not keep:
+        graph.close()
     if wl["algo"] in ("pr_pull",) and "oracle_values" in main:
         main["check"] = (f"all {len(main['values'])} ranks within "
                          f"{pr_check(main['values'], main['oracle_values'], 'pagerank'):.2e} "
@@ -492,7 +519,7 @@ def run_headline(b, args):
         # config 2 as it was meant: 8-byte {dst, w} edges, 40% of them resident
         g.set_edge_packing(False)
         up = b.measure(wl, max(3, args.steps // 2), 3, cpu=False, graph=g,
-                       traffic_key=key + "_unpacked")
+                       traffic_key=traffic_key(wl, packed=False))
         assert np.array_equal(up["values"], ref_vals), "unpacked SSSP differs"
         up["check"] = "all values bit-exact vs the packed run (itself checked vs the CPU oracle)"
         extra["c2_sssp_unpacked"] = public(up)
@@ -503,11 +530,11 @@ def run_headline(b, args):
         gcc = b.gen(wcc)
         lp = b.measure(wcc, args.steps, args.warmup, cpu=not args.no_cpu,
                        run_kw={"label_propagation": True}, graph=gcc,
-                       traffic_key=f"cc_lp_rmat{wl['scale']}_sym_40%", label="cc label propagation")
+                       traffic_key=traffic_key(wcc, label_propagation=True), label="cc label propagation")
         lp["algorithm"] = "min-label propagation (the reference's CC method)"
         extra["c2_cc"] = public(lp)
         uf = b.measure(wcc, args.steps, args.warmup, cpu=False, graph=gcc,
-                       traffic_key=f"cc_uf_rmat{wl['scale']}_sym_40%")
+                       traffic_key=traffic_key(wcc))
         if "oracle_values" in lp:
             assert np.array_equal(uf["values"], lp["oracle_values"]), "union-find CC differs"
             uf["check"] = "all labels bit-exact vs the CPU oracle (min-label fixed point)"
@@ -521,7 +548,7 @@ def run_headline(b, args):
 def run_c1(b, args):
     wl = dict(WORKLOADS["c1"])
     m = b.measure(wl, args.steps, args.warmup, want_e2e=True, cpu=not args.no_cpu,
-                  traffic_key="bfs_rmat20_csr_100%")
+                  traffic_key=traffic_key(wl))
     m["config"] = workload_config(wl, args.source, args.gpus)
     return public(m)
 
@@ -533,7 +560,7 @@ def run_c3(b, args):
     k, w = min(args.steps, 3), 3
     out = {}
     wl = dict(WORKLOADS["c3"])
-    pull = b.measure(wl, k, w, cpu=not args.no_cpu, traffic_key="pr_pull_rmat26_csc_2GiB")
+    pull = b.measure(wl, k, w, cpu=not args.no_cpu, traffic_key=traffic_key(wl))
     ref = pull.pop("oracle_values", None)
     if ref is not None:
         pull["check"] = (f"all {len(ref)} ranks after 20 iterations within "
@@ -542,7 +569,7 @@ def run_c3(b, args):
     pull["config"] = workload_config(wl, None, args.gpus)
     out["c3_pr_pull"] = public(pull)
     wl = dict(WORKLOADS["c3push"])
-    push = b.measure(wl, k, w, cpu=False, traffic_key="pr_push_rmat26_csr_2GiB", keep=True)
+    push = b.measure(wl, k, w, cpu=False, traffic_key=traffic_key(wl), keep=True)
     if ref is not None:
         push["check"] = (f"all {len(ref)} ranks after 20 iterations within "
                          f"{pr_check(push['values'], ref, 'pr_push'):.2e} relative of the FP64 "
@@ -624,8 +651,9 @@ def stream_plain(g, algos, src, arr):
     return len(src) / (time.perf_counter() - t0), np.array(lat) * 1e3, sums
 
 
-def stream_served(T, g, algos, src, arr, group_min):
-    with T.Server(g, max_slots=64, group_min=group_min) as sv:
+def stream_served(T, g, algos, src, arr, group_min, join_window=0, groups_per_algo=0):
+    with T.Server(g, max_slots=64, group_min=group_min, join_window=join_window,
+                  groups_per_algo=groups_per_algo) as sv:
         t0 = time.perf_counter()
         tickets = []
         for i, (a, s_) in enumerate(zip(algos, src)):
@@ -672,7 +700,8 @@ def run_c5(b, args):
         if answers is None:
             answers = psum
         assert psum == answers, "plain stream answers differ between rates"
-        sq, stats = stream_served(T, g, algos, src, arr, args.group_min)
+        sq, stats = stream_served(T, g, algos, src, arr, args.group_min, args.join_window,
+                                  args.groups_per_algo)
         for i, st in enumerate(stats):
             assert st["checksum"] == answers[i], f"c5 query {i} ({algos[i]} {src[i]}) differs"
         slat = np.array([st["latency_ms"] for st in stats])

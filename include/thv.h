@@ -320,6 +320,15 @@ typedef struct thv_serve_opts {
   uint32_t replan_every;     /* re-place the graph's blocks by measured
                                 access (THV_PLACE_ACCESS, same budget) after
                                 this many finished queries; 0 = never */
+  uint32_t join_window;      /* batching: a running group admits arrivals
+                                during its first join_window iterations
+                                only (later ones start or wait for another
+                                group); 0 = default (2); 0xFFFFFFFF = for
+                                its whole life */
+  uint32_t groups_per_algo;  /* batching: groups of one algorithm on the
+                                device at once (1 or 2): with 2, a second
+                                group starts for arrivals while the first
+                                one drains (the two take turns); 0 = 1 */
 } thv_serve_opts;
 
 typedef struct thv_query_stats {

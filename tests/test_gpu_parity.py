@@ -139,6 +139,25 @@ def test_pagerank_pull(T, O, g14, frac):
         assert max_rel(got, want) <= PR_RTOL
 
 
+@pytest.mark.parametrize("frac", [0.0, 0.4])
+def test_pagerank_scale20_twenty_iterations_every_vertex(T, O, frac):
+    # config-3 shape at scale 20 (1 M vertices, 16 M edges, hub in-degrees in
+    # the thousands): pull over the CSC and push over the CSR of the same
+    # graph, 20 iterations, every vertex against one FP64 oracle run, with
+    # part (or none) of the edges resident and the rest read over the link
+    g = O.rmat(20, 16)
+    io, ia, od = O.transpose(g)
+    want = O.pagerank_csc(io, ia, od, 20)
+    with T.Graph.from_arrays(io, ia, "csc", outdeg=od) as eg:
+        eg.plan(int(frac * eg.ne * 4), small_list_degree=1)
+        got, _ = eg.run("pr_pull", pr_iters=20)
+        assert max_rel(got, want) <= PR_RTOL
+    with T.Graph.from_arrays(g.off, g.adj, "csr") as eg:
+        eg.plan(int(frac * eg.ne * 4), small_list_degree=1)
+        got, _ = eg.run("pr_push", pr_iters=20)
+        assert max_rel(got, want) <= PR_RTOL
+
+
 def test_pagerank_hub_split_tiles(T, O):
     # one vertex with in/out-degree 20000 (> tile size): split tiles
     n = 30000

@@ -1,6 +1,7 @@
 """Serving: continuous batching.  Every query's result equals the single
--source run bit for bit, whether it ran alone or joined a traversal that
-other queries already occupied (admitted into a freed slot mid-stream)."""
+-source run bit for bit, whether it ran alone, started a batched group,
+joined a batched group already on the device (into a freed mask bit), or
+joined a slot traversal mid-stream."""
 import time
 
 import numpy as np
@@ -184,13 +185,15 @@ def graph_with_tail(O, T, tail, seed_scale=14):
 
 @pytest.mark.parametrize("algo,tail", [("sssp", 6000), ("bfs", 100)])
 def test_arrival_joins_a_running_batched_group(T, O, algo, tail):
-    # group_min 1: the first query starts a batched group at once; queries
-    # submitted while it runs must join it mid-flight (grouped 1, joined 1)
-    # with the answer of their solo run
+    # group_min 1: the first query starts a batched group at once; with the
+    # join window open for the group's whole life, queries submitted while
+    # it runs must join it mid-flight (grouped 1, joined 1) with the answer
+    # of their solo run
     gp, eg, hub = graph_with_tail(O, T, tail)
     late = [int(x) for x in O.sources(gp, 40)][:4]
     try:
-        with T.Server(eg, group_min=1, max_batch_iters=1, timeout_ms=20000) as sv:
+        with T.Server(eg, group_min=1, max_batch_iters=1, join_window=0xFFFFFFFF,
+                      timeout_ms=20000) as sv:
             first = sv.submit(algo, hub)
             time.sleep(0.002)
             tickets = []
@@ -213,13 +216,53 @@ def test_arrival_joins_a_running_batched_group(T, O, algo, tail):
         eg.close()
 
 
+def test_arrivals_after_the_join_window_start_a_second_group(T, O):
+    # default join window (2 iterations), two groups per algorithm: a query
+    # arriving after the window starts a second group at once, which shares
+    # the device with the first by turns, instead of waiting for the first
+    # group to drain
+    gp, eg, hub = graph_with_tail(O, T, 6000)
+    late = [int(x) for x in O.sources(gp, 40)][:4]
+    try:
+        with T.Server(eg, group_min=1, max_batch_iters=1, groups_per_algo=2,
+                      timeout_ms=20000) as sv:
+            first = sv.submit("sssp", hub)
+            time.sleep(0.005)
+            tickets = [(sv.submit("sssp", s), s) for s in late]
+            vals, st0 = sv.wait(first)
+            assert np.array_equal(vals, O.sssp(gp, hub))
+            for j, (t, s) in enumerate(tickets):
+                vals, st = sv.wait(t)
+                assert np.array_equal(vals, O.sssp(gp, s)), s
+                assert st["grouped"] == 1
+                if j == 0:
+                    assert st["queue_ms"] < st0["run_ms"] / 2, (st, st0)
+    finally:
+        eg.close()
+
+
+@pytest.mark.parametrize("groups", [1, 2])
+def test_one_or_two_groups_per_algorithm_agree(T, O, g14w, eg, groups):
+    src = O.sources(g14w, 90).tolist()
+    algos = ["sssp" if i % 4 == 0 else "bfs" for i in range(len(src))]
+    with T.Server(eg, groups_per_algo=groups, timeout_ms=20000) as sv:
+        tickets = []
+        for i, (a, s) in enumerate(zip(algos, src)):
+            tickets.append(sv.submit(a, s, want_values=False))
+            if i % 8 == 0:
+                time.sleep(0.001)
+        for t, a, s in zip(tickets, algos, src):
+            _, st = sv.wait(t)
+            assert st["checksum"] == T.values_checksum(want(O, g14w, a, s)), (a, s)
+
+
 def test_joined_sources_reuse_freed_bits(T, O):
     # a long stream through one live group: more queries than mask bits, so
     # bits of finished sources are reset and reused by later arrivals
     gp, eg, hub = graph_with_tail(O, T, 120)
     src = [int(x) for x in O.sources(gp, 150)]
     try:
-        with T.Server(eg, group_min=1, timeout_ms=20000) as sv:
+        with T.Server(eg, group_min=1, join_window=0xFFFFFFFF, timeout_ms=20000) as sv:
             tickets = []
             for i, s in enumerate(src):
                 tickets.append((sv.submit("bfs" if i % 3 else "sssp", s, want_values=(i % 7 == 0)), s, i))

@@ -102,7 +102,8 @@ class _ServeOpts(ctypes.Structure):
     _fields_ = [("max_slots", ctypes.c_uint32), ("queue_capacity", ctypes.c_uint32),
                 ("mem_budget_bytes", ctypes.c_uint64), ("timeout_ms", ctypes.c_uint32),
                 ("max_batch_iters", ctypes.c_uint32), ("group_min", ctypes.c_uint32),
-                ("replan_every", ctypes.c_uint32)]
+                ("replan_every", ctypes.c_uint32), ("join_window", ctypes.c_uint32),
+                ("groups_per_algo", ctypes.c_uint32)]
 
 
 class _QueryStats(ctypes.Structure):
@@ -424,7 +425,8 @@ class Server:
 
     def __init__(self, graph: Graph, max_slots: int = 64, queue_capacity: int = 0,
                  mem_budget_bytes: int = 0, timeout_ms: int = 0, max_batch_iters: int = 0,
-                 group_min: int = 0, replan_every: int = 0):
+                 group_min: int = 0, replan_every: int = 0, join_window: int = 0,
+                 groups_per_algo: int = 0):
         """group_min: waiting queries of one algorithm that run as a batched
         group (0 = measured defaults: BFS 4, SSSP 6; 0xFFFFFFFF = no
         batching: slot admission)."""
@@ -432,7 +434,7 @@ class Server:
         self.graph = graph
         self._bufs = {}
         o = _ServeOpts(max_slots, queue_capacity, mem_budget_bytes, timeout_ms, max_batch_iters,
-                       group_min, replan_every)
+                       group_min, replan_every, join_window, groups_per_algo)
         self._h = ctypes.c_void_p()
         _check(lib.thv_serve_start(graph._h, ctypes.byref(o), ctypes.byref(self._h)),
                "thv_serve_start")

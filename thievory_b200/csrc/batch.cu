@@ -1061,6 +1061,8 @@ void batch_free(thv_graph *g) {
 // configuration may use, so tuning never reallocates.  BFS and SSSP keep
 // separate states, so alternating between them (served groups) does not
 // reallocate either.
+static thv_status fill_batch_state(thv_graph *g, BatchState *b, bool sssp, bool want_out);
+
 static thv_status ensure_batch_state(thv_graph *g, bool sssp, bool want_out) {
   BatchState *&b = g->bs_keep[sssp ? 1 : 0];
   g->bs = nullptr;
@@ -1071,6 +1073,11 @@ static thv_status ensure_batch_state(thv_graph *g, bool sssp, bool want_out) {
   free_state(b);
   b = new BatchState();
   g->bs = b;
+  return fill_batch_state(g, b, sssp, want_out);
+}
+
+// Allocates every buffer of b (b->valid once all succeeded).
+static thv_status fill_batch_state(thv_graph *g, BatchState *b, bool sssp, bool want_out) {
   b->nv = g->nv;
   b->sssp = sssp;
   const uint64_t nw = (g->nv + 31) / 32;
@@ -1475,9 +1482,8 @@ static MsArgs live_args(thv_graph *g, const LiveGroup *lg, uint32_t timeout_ms) 
 }
 
 static thv_status live_state(thv_graph *g, const LiveGroup *lg) {
-  BatchState *b = g->bs_keep[lg->sssp ? 1 : 0];
-  if (!b || !b->valid) return fail(THV_EINVAL, "live group has no batch state");
-  g->bs = b;
+  if (!lg->bs || !lg->bs->valid) return fail(THV_EINVAL, "live group has no batch state");
+  g->bs = lg->bs;
   return THV_OK;
 }
 
@@ -1489,10 +1495,14 @@ thv_status live_open(thv_graph *g, LiveGroup *lg, bool sssp) {
   THV_TRY(pinned_alloc((void **)&lg->h_buf, 4 * kMsWidth * 4, "live group staging"));
   THV_TRY(dev_alloc((void **)&lg->d_sums, kMsWidth * 8, "live group checksums"));
   THV_TRY(pinned_alloc((void **)&lg->h_sums, kMsWidth * 8, "live group checksums"));
-  return ensure_batch_state(g, sssp, false);
+  // each live group owns its traversal state, so several can be on the
+  // device at once (the graph's own batch states serve thv_batch_run)
+  lg->bs = new BatchState();
+  return fill_batch_state(g, lg->bs, sssp, false);
 }
 
 void live_close(LiveGroup *lg) {
+  free_state(lg->bs);
   dev_free(lg->d_buf);
   pinned_free(lg->h_buf);
   dev_free(lg->d_sums);
@@ -1517,7 +1527,6 @@ thv_status live_add(thv_graph *g, LiveGroup *lg, uint32_t k, const uint32_t *sou
     return fail(THV_EINVAL, "live group: %u sources do not fit", k);
   const bool fresh = !lg->running;
   if (fresh) {
-    THV_TRY(ensure_batch_state(g, lg->sssp, false));
     MsConfig cfg = kMsDefault;
     tune_lookup(tune_key(g, lg->sssp), &cfg);  // a configuration tuned by thv_batch_run
     lg->small = cfg.small;

@@ -99,7 +99,8 @@ struct MinCtrl {
 struct MinArgs {
   uint32_t *val;
   uint32_t *bm;
-  uint32_t *wmin;  // SSSP: lower bound of the pending values in each bitmap word
+  uint32_t *wmin;  // SSSP/CC: lower bound of the pending values in each bitmap word;
+                   // BFS (may be null): per-group counters of the compaction
   const uint64_t *off;
   const uint32_t *blk_vb;
   const uint64_t *blk_base;
@@ -145,6 +146,21 @@ struct MinState {
   bool valid = false;
 };
 
+// Position of the n-th (from 0) set bit of x; n < popc(x).
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t n) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t s = 16; s > 0; s >>= 1) {
+    const uint32_t lo = __popc(x & ((1u << s) - 1u));
+    if (n >= lo) {
+      n -= lo;
+      x >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
 template <int OP>
 __device__ __forceinline__ void activate(const MinArgs &a, uint32_t w,
                                          unsigned long long cand) {
@@ -154,20 +170,50 @@ __device__ __forceinline__ void activate(const MinArgs &a, uint32_t w,
   if (!(ldcg(bp) & m)) atomicOr(bp, m);
 }
 
+// Direction-optimising BFS keeps the frontier double-buffered: a vertex
+// found at this level goes into `bits` (the next level's bitmap), and the
+// next level's size and out-edges are counted as vertices are found, so the
+// next level's direction is known before any of its work.
+struct NextLevel {
+  uint32_t *bits;
+  unsigned long long nf, mf;
+};
+
 // Relax N edges at once: all value probes are issued before any atomic so a
-// lane keeps N loads in flight.
-template <int OP, int N>
+// lane keeps N loads in flight.  NEXT (BFS): mark found vertices in nl->bits
+// and count them and their out-edges.
+template <int OP, int N, bool NEXT = false>
 __device__ __forceinline__ void relax_n(const MinArgs &a, const uint32_t (&w)[N],
                                         const unsigned long long (&cand)[N],
-                                        const bool (&ok)[N]) {
+                                        const bool (&ok)[N], NextLevel *nl = nullptr) {
   uint32_t cur[N];
 #pragma unroll
   for (int j = 0; j < N; j++) cur[j] = ok[j] ? ldcg(a.val + w[j]) : 0u;
+  if constexpr (NEXT) {
+    bool found[N];
 #pragma unroll
-  for (int j = 0; j < N; j++) {
-    if (ok[j] && cand[j] < cur[j]) {
-      const uint32_t old = atomicMin(a.val + w[j], (uint32_t)cand[j]);
-      if (cand[j] < old) activate<OP>(a, w[j], cand[j]);
+    for (int j = 0; j < N; j++)
+      found[j] = ok[j] && cand[j] < cur[j] && cand[j] < atomicMin(a.val + w[j], (uint32_t)cand[j]);
+    uint32_t deg[N];
+#pragma unroll
+    for (int j = 0; j < N; j++)
+      deg[j] = found[j] ? (uint32_t)(__ldg(a.off + w[j] + 1) - __ldg(a.off + w[j])) : 0u;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      if (!found[j]) continue;
+      const uint32_t m = 1u << (w[j] & 31u);
+      uint32_t *bp = nl->bits + (w[j] >> 5);
+      if (!(ldcg(bp) & m)) atomicOr(bp, m);
+      nl->nf++;
+      nl->mf += deg[j];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      if (ok[j] && cand[j] < cur[j]) {
+        const uint32_t old = atomicMin(a.val + w[j], (uint32_t)cand[j]);
+        if (cand[j] < old) activate<OP>(a, w[j], cand[j]);
+      }
     }
   }
 }
@@ -183,15 +229,21 @@ __device__ __forceinline__ unsigned long long candidate(uint32_t vval, uint32_t 
                          : (unsigned long long)vval;
 }
 
-// One high-degree chunk per warp: 128-byte aligned 16-byte loads, two per
-// lane in flight, lanes outside [start, end) masked.
-template <int OP, int ESZ>
-__device__ __forceinline__ void process_chunk(const MinArgs &a, const MinItem &it) {
+// One high-degree chunk (or part `part` of `parts` of it) per warp:
+// 128-byte aligned 16-byte loads, two per lane in flight, lanes outside
+// [start, end) masked.
+template <int OP, int ESZ, bool NEXT = false>
+__device__ __forceinline__ void process_chunk(const MinArgs &a, const MinItem &it, unsigned part,
+                                              unsigned parts, NextLevel *nl = nullptr) {
   constexpr int PER = 16 / ESZ;  // edges per 16-byte load
   const unsigned lane = lane_id();
   const uint32_t vval = it.val;
-  const uintptr_t start = it.ea_cnt & kAddrMask;
-  const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
+  const uint32_t cnt = (uint32_t)(it.ea_cnt >> 48);
+  // parts of whole 32-edge runs
+  const uint32_t per = ((cnt + parts - 1) / parts + 31u) & ~31u;
+  const uint32_t lo = min(cnt, part * per), hi = min(cnt, lo + per);
+  const uintptr_t start = (it.ea_cnt & kAddrMask) + (uintptr_t)lo * ESZ;
+  const uintptr_t end = (it.ea_cnt & kAddrMask) + (uintptr_t)hi * ESZ;
   for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; p < end; p += 1024u) {
     uint4 q[2];
     q[0] = ld_nc_v4(p);
@@ -213,33 +265,39 @@ __device__ __forceinline__ void process_chunk(const MinArgs &a, const MinItem &i
         cand[k] = candidate<OP>(vval, ESZ == 4 ? edge_wt(f[j], a.wshift, a.wbase) : f[2 * j + 1]);
       }
     }
-    relax_n<OP, 2 * PER>(a, w, cand, ok);
+    relax_n<OP, 2 * PER, NEXT>(a, w, cand, ok, nl);
   }
 }
 
-// 32 low-degree vertices per warp: warp-cooperative load balancing over
-// their concatenated adjacency, 64 edges per step (two per lane in flight).
-template <int OP, int ESZ>
+// Scan-mode small-vertex groups: edges per lane in flight per step.
+constexpr int kScanGroupPer = 4;
+
+// Up to 32 (gsize) low-degree vertices per warp: warp-cooperative load
+// balancing over their concatenated adjacency, kScanGroupPer x 32 edges per
+// step (each lane's edges in flight together).
+template <int OP, int ESZ, bool NEXT = false>
 __device__ __forceinline__ void process_group(const MinArgs &a, unsigned long long first,
-                              unsigned long long n_small) {
+                              unsigned long long n_small, unsigned gsize = 32,
+                              NextLevel *nl = nullptr) {
+  constexpr int P = kScanGroupPer;
   const unsigned lane = lane_id();
   const unsigned long long idx = first + lane;
   MinItem it{0, 0, 0};
-  if (idx < n_small) it = a.qs[idx];
+  if (lane < gsize && idx < n_small) it = a.qs[idx];
   const uint32_t vval = it.val;
   const unsigned cnt = (unsigned)(it.ea_cnt >> 48);
   const unsigned long long eaddr = it.ea_cnt & kAddrMask;
   const unsigned incl = warp_incl_scan<unsigned>(cnt);
   const unsigned excl = incl - cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
-  for (unsigned k = 0; k < total; k += 64) {
-    uint32_t w[2];
-    unsigned long long cand[2];
-    bool ok[2];
-    uintptr_t addr[2];
-    uint32_t ov[2];
+  for (unsigned k = 0; k < total; k += 32u * P) {
+    uint32_t w[P];
+    unsigned long long cand[P];
+    bool ok[P];
+    uintptr_t addr[P];
+    uint32_t ov[P];
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
+    for (int h = 0; h < P; h++) {
       const unsigned t = k + 32u * h + lane;
       const int o = warp_owner(excl, t);
       const unsigned long long ea = shfl64(eaddr, o);
@@ -248,9 +306,9 @@ __device__ __forceinline__ void process_group(const MinArgs &a, unsigned long lo
       ok[h] = t < total;
       addr[h] = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
     }
-    uint32_t wt[2] = {0, 0};
+    uint32_t wt[P];
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
+    for (int h = 0; h < P; h++) {
       if (ESZ == 4) {
         const uint32_t e = ok[h] ? ld_nc_u32(addr[h]) : 0u;
         w[h] = edge_dst(e, a.wshift);
@@ -262,26 +320,29 @@ __device__ __forceinline__ void process_group(const MinArgs &a, unsigned long lo
       }
     }
 #pragma unroll
-    for (int h = 0; h < 2; h++) cand[h] = candidate<OP>(ov[h], wt[h]);
-    relax_n<OP, 2>(a, w, cand, ok);
+    for (int h = 0; h < P; h++) cand[h] = candidate<OP>(ov[h], wt[h]);
+    relax_n<OP, P, NEXT>(a, w, cand, ok, nl);
   }
 }
 
 // Bottom-up BFS level: every unreached vertex scans its in-edges for a
-// parent in this level's frontier (the copy in bm2), stopping at the first.
-// A warp owns 32 vertices (one bitmap word) at a time, so the next frontier
-// word is its ballot, stored whole into bm (empty after the compaction).
-// value = level + 1 for the vertices reached here.
+// parent in this level's frontier `front`, stopping at the first.  A warp
+// owns 32 vertices (one bitmap word) at a time, so the next frontier word is
+// its ballot, stored whole into `next`.  value = level + 1 for the vertices
+// reached here; their number and out-edges go to *next_nf / *next_mf.
 // (Scalar arguments: a MinArgs reference would copy the kernel's
 // parameter block to local memory.)
 __device__ __noinline__ void bfs_bottom_up(const uint64_t *in_off, const uint32_t *in_adj,
-                                           const uint32_t *front, uint32_t *next, uint32_t *val,
-                                           uint32_t nv, uint32_t value,
-                                           unsigned long long *edges, unsigned long long *level_scan,
-                                           unsigned gwarp, unsigned nwarps) {
+                                           const uint64_t *off, const uint32_t *front,
+                                           uint32_t *next, uint32_t *val, uint32_t nv,
+                                           uint32_t value, unsigned long long *edges,
+                                           unsigned long long *level_scan,
+                                           unsigned long long *next_nf,
+                                           unsigned long long *next_mf, unsigned gwarp,
+                                           unsigned nwarps) {
   const unsigned lane = lane_id();
   const uint32_t nwords = (nv + 31) / 32;
-  unsigned long long scanned = 0;
+  unsigned long long scanned = 0, nf = 0, mf = 0;
   for (uint32_t w = gwarp; w < nwords; w += nwarps) {
     const uint32_t v = w * 32u + lane;
     bool found = false;
@@ -295,16 +356,206 @@ __device__ __noinline__ void bfs_bottom_up(const uint64_t *in_off, const uint32_
           break;
         }
       }
-      if (found) val[v] = value;
+      if (found) {
+        val[v] = value;
+        nf++;
+        mf += __ldg(off + v + 1) - __ldg(off + v);
+      }
     }
     const unsigned fm = __ballot_sync(kFull, found);
-    if (lane == 0 && fm) next[w] = fm;
+    if (lane == 0) next[w] = fm;
   }
   scanned = warp_sum(scanned);
-  if (lane == 0 && scanned) {
-    atomicAdd(edges, scanned);
-    atomicAdd(level_scan, scanned);
+  nf = warp_sum(nf);
+  mf = warp_sum(mf);
+  if (lane == 0) {
+    if (scanned) {
+      atomicAdd(edges, scanned);
+      atomicAdd(level_scan, scanned);
+    }
+    if (nf) {
+      atomicAdd(next_nf, nf);
+      atomicAdd(next_mf, mf);
+    }
   }
+}
+
+// Direction-optimising BFS on a graph whose out-edges are all resident,
+// with an in-edge transpose in HBM.  The frontier is double-buffered (F:
+// this level's, N: the next one's), and each level's direction is decided
+// before any of its work, from its frontier's size and out-edges, which the
+// previous level counted while it found those vertices (Beamer et al.,
+// SC'12: bottom-up when the frontier's out-edges exceed the unexplored
+// edges / alpha; top-down again when the frontier holds fewer than nv / beta
+// vertices, or its out-edges fall below half of what the last bottom-up
+// level scanned).  A top-down level compacts F into work queues (clearing N
+// on the way) and expands them, marking found vertices in N: two grid
+// barriers.  A bottom-up level is one sweep that writes N whole: one
+// barrier, and no compaction at all.  Levels are unique, so the values are
+// bit-exact whatever the direction.
+template <int ESZ>
+__global__ void __launch_bounds__(kMinThreads, 2) bfs_do_kernel(MinArgs a) {
+  extern __shared__ unsigned long long s_tab[];
+  const bool smem_tab = a.nblk <= kSmemBlocks;
+  unsigned long long *s_base = s_tab;
+  uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_tab + a.nblk);
+  if (smem_tab) {
+    for (uint32_t i = threadIdx.x; i <= a.nblk; i += blockDim.x) s_vb[i] = a.blk_vb[i];
+    for (uint32_t i = threadIdx.x; i < a.nblk; i += blockDim.x) s_base[i] = a.blk_base[i];
+  }
+  __syncthreads();
+  const uint32_t *vb = smem_tab ? s_vb : a.blk_vb;
+  const unsigned long long *bbase = smem_tab ? s_base : (const unsigned long long *)a.blk_base;
+  MinCtrl *c = a.ctrl;
+  const unsigned lane = lane_id();
+  const unsigned gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  // fewer bitmap groups than warps: nsub warps share a group, each taking
+  // every nsub-th step of its numbered vertices (F is only read here)
+  const unsigned nsub = a.ngroups * 2u <= nwarps ? min(8u, nwarps / a.ngroups) : 1u;
+  const unsigned gstride = nwarps / nsub, sub = gwarp % nsub;
+  uint32_t *F = a.bm, *N = a.bm2;
+  unsigned long long mu = a.ne;      // out-edges of vertices not yet reached
+  unsigned long long last_scan = 0;  // in-edges scanned by the last bottom-up level
+  bool bottom_up = false;
+  const unsigned long long src_deg = __ldg(a.off + a.src + 1) - __ldg(a.off + a.src);
+  unsigned iter = 0;
+  for (;; ++iter) {
+    if (iter >= a.max_iters) {
+      if (leader) atomicCAS(&c->err, 0u, kDevErrIters);
+      break;
+    }
+    // Counter slots.  Level L compacts into slot L % 3 and counts level
+    // L+1's frontier into (L + 1) % 3, which is read at the top of level
+    // L + 1.  Slot (L + 2) % 3 of those counters was last read before level
+    // L - 1's last barrier and is next written during level L + 1, so it is
+    // cleared now.  The bottom-up scan count of level L (slot L % 3) is read
+    // just after level L's last barrier, so it is cleared one level ahead
+    // instead: slot (L + 1) % 3, last read after level L - 2's barrier.
+    const unsigned slot = iter % 3, nslot = (iter + 1) % 3, zslot = (iter + 2) % 3;
+    if (leader) {
+      c->cnt_small[zslot] = 0;
+      c->cnt_big[zslot] = 0;
+      c->wc[zslot] = 0;
+      c->mf[zslot] = 0;
+      c->nf[zslot] = 0;
+      c->bu_scan[nslot] = 0;
+    }
+    const unsigned long long nf = iter == 0 ? 1ull : ldcg(&c->nf[slot]);
+    const unsigned long long mf = iter == 0 ? src_deg : ldcg(&c->mf[slot]);
+    if (nf == 0) break;
+    mu = mu > mf ? mu - mf : 0;
+    bottom_up = bottom_up ? nf * a.do_beta >= a.nv && 2 * mf > last_scan : mf * a.do_alpha > mu;
+    const uint32_t lval = iter + 1u;  // value of this level's vertices
+    if (bottom_up) {
+      bfs_bottom_up(a.in_off, a.in_adj, a.off, F, N, a.val, a.nv, lval + 1u, &c->edges,
+                    &c->bu_scan[slot], &c->nf[nslot], &c->mf[nslot], gwarp, nwarps);
+      if (leader) c->bu_levels++;
+      if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+      last_scan = ldcg(&c->bu_scan[slot]);
+    } else {
+      if (leader) atomicAdd(&c->edges, mf);
+      // ------------------------------------------------------ compaction
+      unsigned long long my_hbm = 0, my_link = 0;
+      for (unsigned g = gwarp / nsub; g < a.ngroups && gwarp / nsub < gstride; g += gstride) {
+        const unsigned wbase = g * 32u;
+        const uint32_t word = ldcg(F + wbase + lane);
+        if (sub == 0) N[wbase + lane] = 0;
+        const unsigned cnt = (unsigned)__popc(word);
+        const unsigned incl = warp_incl_scan<unsigned>(cnt);
+        const unsigned excl = incl - cnt, total = __shfl_sync(kFull, incl, 31);
+        for (unsigned k = 32u * sub; k < total; k += 32u * nsub) {
+          const unsigned t = k + lane;
+          const int own = warp_owner(excl, t);
+          const uint32_t ow = __shfl_sync(kFull, word, own);
+          const unsigned oex = __shfl_sync(kFull, excl, own);
+          const bool take = t < total;
+          const uint32_t v = take ? (wbase + own) * 32u + nth_set_bit(ow, t - oex) : 0u;
+          uint32_t deg = 0;
+          unsigned long long eaddr = 0;
+          if (take) {
+            const uint64_t s0 = __ldg(a.off + v), e0 = __ldg(a.off + v + 1);
+            deg = (uint32_t)(e0 - s0);
+            bool host;
+            const uint32_t bi = find_block(vb, a.nblk, v);
+            eaddr = list_addr(a.lc, bbase[bi], a.host_base, v, s0, deg, ESZ, &host);
+            if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
+            if (host) my_link += (unsigned long long)deg * ESZ;
+            else my_hbm += (unsigned long long)deg * ESZ;
+          }
+          const bool small = take && deg > 0 && deg < a.small_deg;
+          const bool big = take && deg >= a.small_deg;
+          const unsigned sm = __ballot_sync(kFull, small);
+          if (sm) {
+            const int ldr = __ffs(sm) - 1;
+            unsigned long long base = 0;
+            if (lane == (unsigned)ldr)
+              base = atomicAdd(&c->cnt_small[slot], (unsigned long long)__popc(sm));
+            base = shfl64(base, ldr);
+            const unsigned long long pos = base + __popc(sm & lanemask_lt());
+            if (small) {
+              if (pos < a.cap_s) a.qs[pos] = make_item(eaddr, deg, v, lval);
+              else atomicCAS(&c->err, 0u, kDevErrQueue);
+            }
+          }
+          if (__any_sync(kFull, big)) {
+            const unsigned nch = big ? (deg + a.chunk - 1) / a.chunk : 0u;
+            const unsigned inc = warp_incl_scan<unsigned>(nch);
+            const unsigned tot = __shfl_sync(kFull, inc, 31);
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(&c->cnt_big[slot], (unsigned long long)tot);
+            base = shfl64(base, 0);
+            if (big) {
+              unsigned long long pos = base + inc - nch;
+              for (unsigned kk = 0; kk < nch; kk++, pos++) {
+                const uint32_t lo = kk * a.chunk;
+                if (pos < a.cap_b)
+                  a.qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, min(a.chunk, deg - lo), v, lval);
+                else
+                  atomicCAS(&c->err, 0u, kDevErrQueue);
+              }
+            }
+          }
+        }
+      }
+      my_hbm = warp_sum(my_hbm);
+      my_link = warp_sum(my_link);
+      if (lane == 0 && my_hbm + my_link) {
+        atomicAdd(&c->hbm_bytes, my_hbm);
+        atomicAdd(&c->link_bytes, my_link);
+      }
+      if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+      // ------------------------------------------------------- expansion
+      const unsigned long long ns = ldcg(&c->cnt_small[slot]);
+      const unsigned long long nb = ldcg(&c->cnt_big[slot]);
+      unsigned gsize = 32;
+      while (gsize > 4 && nb + (ns + gsize - 1) / gsize < nwarps / 2) gsize >>= 1;
+      const unsigned long long ngrp = (ns + gsize - 1) / gsize;
+      const unsigned parts =
+          nb && nb + ngrp < nwarps ? (unsigned)min(8ull, max(1ull, (nwarps - ngrp) / nb)) : 1u;
+      const unsigned long long nbt = nb * parts, ntask = nbt + ngrp;
+      NextLevel nl{N, 0, 0};
+      for (unsigned long long t = gwarp; t < ntask;) {
+        unsigned long long nt = 0;
+        if (lane == 0) nt = atomicAdd(&c->wc[slot], 1ull);
+        if (t < nbt) process_chunk<OP_BFS, ESZ, true>(a, a.qb[t / parts], (unsigned)(t % parts), parts, &nl);
+        else process_group<OP_BFS, ESZ, true>(a, (t - nbt) * gsize, ns, gsize, &nl);
+        t = nwarps + shfl64(nt, 0);
+      }
+      nl.nf = warp_sum(nl.nf);
+      nl.mf = warp_sum(nl.mf);
+      if (lane == 0 && nl.nf) {
+        atomicAdd(&c->nf[nslot], nl.nf);
+        atomicAdd(&c->mf[nslot], nl.mf);
+      }
+      if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+    }
+    uint32_t *x = F;
+    F = N;
+    N = x;
+  }
+  if (leader) c->iters = iter;
 }
 
 template <int OP, int ESZ>
@@ -312,6 +563,7 @@ __global__ void __launch_bounds__(kMinThreads)
     minprop_kernel(MinArgs a) {
   // block table (first vertex, base address) in shared memory when it fits
   extern __shared__ unsigned long long s_tab[];
+  __shared__ uint32_t s_word[kMinThreads / 32][64];  // compaction: taken bits, least kept value per word
   const bool smem_tab = a.nblk <= kSmemBlocks;
   unsigned long long *s_base = s_tab;
   uint32_t *s_vb = reinterpret_cast<uint32_t *>(s_tab + a.nblk);
@@ -336,10 +588,6 @@ __global__ void __launch_bounds__(kMinThreads)
   uint32_t width = a.delta;
   if (OP == OP_SSSP) thr = (uint32_t)min(1ull + a.delta, 0xFFFFFFFFull);
   if (OP == OP_CC) thr = a.delta;
-  unsigned long long mu = a.ne;  // BFS: out-edges of vertices not yet reached
-  unsigned long long last_scan = 0;  // in-edges scanned by the last bottom-up level
-  bool bottom_up = false;
-
   unsigned iter = 0;
   for (;; ++iter) {
     if (iter >= a.max_iters) {
@@ -358,16 +606,29 @@ __global__ void __launch_bounds__(kMinThreads)
       c->bu_scan[nslot] = 0;
     }
     // ---------------------------------------------------------- compaction
+    // A warp owns 32 bitmap words (lane = word).  The pending vertices of
+    // its words are numbered across the warp and handled 32 per step (lane =
+    // vertex), however they are spread over the words, so a group costs
+    // ceil(pending / 32) steps instead of one step per non-empty word;
+    // per-word results (taken bits, least kept value) gather in shared
+    // memory and each word is rewritten once.  Queue items come out in
+    // vertex order.
     unsigned long long my_edges = 0, my_hbm = 0, my_link = 0, my_verts = 0;
     unsigned long long my_keep = 0;
     uint32_t my_min = 0xFFFFFFFFu;
-    for (unsigned g = gwarp; g < a.ngroups; g += nwarps) {
+    uint32_t *s_tk = s_word[threadIdx.x >> 5], *s_km = s_tk + 32;
+    // Fewer groups than warps (small graphs): BFS shares each group among
+    // nsub warps, each taking every nsub-th step of the group's numbered
+    // vertices.  BFS takes every pending vertex, so the group's words end
+    // up empty; the last of its warps to finish (a per-group counter that
+    // wraps back to 0) clears them, after every one of them has read them.
+    const unsigned nsub =
+        OP == OP_BFS && a.wmin && a.ngroups * 2u <= nwarps ? min(8u, nwarps / a.ngroups) : 1u;
+    const unsigned gstride = nwarps / nsub, sub = gwarp % nsub;
+    for (unsigned g = gwarp / nsub; g < a.ngroups && gwarp / nsub < gstride; g += gstride) {
       const unsigned wbase = g * 32u;
       const uint32_t word = ldcg(a.bm + wbase + lane);
-      // BFS with a transpose: keep this level's frontier for a bottom-up
-      // sweep (zero words too, clearing the previous level's copy)
-      if (OP == OP_BFS && a.do_alpha) a.bm2[wbase + lane] = word;
-      unsigned nz = __ballot_sync(kFull, word != 0);
+      bool act_word = word != 0;
       if (OP != OP_BFS) {
         // a word whose pending values are all >= thr is kept without
         // touching its vertices
@@ -375,41 +636,44 @@ __global__ void __launch_bounds__(kMinThreads)
         if (word != 0 && wm >= thr) {
           my_keep += __popc(word);
           my_min = min(my_min, wm);
+          act_word = false;
         }
-        nz = __ballot_sync(kFull, word != 0 && wm < thr);
       }
-      while (nz) {
-        const int j = __ffs(nz) - 1;
-        nz &= nz - 1;
-        const uint32_t wd = __shfl_sync(kFull, word, j);
-        const uint32_t v = (wbase + j) * 32u + lane;
-        const bool act = (wd >> lane) & 1u;
-        bool take = act;
-        uint32_t vval = 0;
-        if (OP != OP_BFS && act) {
-          vval = ldcg(a.val + v);
-          take = vval < thr;
+      const unsigned cnt = act_word ? (unsigned)__popc(word) : 0u;
+      const unsigned incl = warp_incl_scan<unsigned>(cnt);
+      const unsigned excl = incl - cnt, total = __shfl_sync(kFull, incl, 31);
+      if (total == 0) continue;
+      s_tk[lane] = 0;
+      s_km[lane] = 0xFFFFFFFFu;
+      __syncwarp();
+      for (unsigned k = 32u * sub; k < total; k += 32u * nsub) {
+        const unsigned t = k + lane;
+        const int own = warp_owner(excl, t);
+        const uint32_t ow = __shfl_sync(kFull, word, own);
+        const unsigned oex = __shfl_sync(kFull, excl, own);
+        const bool in = t < total;
+        const uint32_t v = in ? (wbase + own) * 32u + nth_set_bit(ow, t - oex) : 0u;
+        uint64_t s0 = 0, e0 = 0;
+        // BFS takes every pending vertex: its offsets load beside its value
+        if (OP == OP_BFS && in) {
+          s0 = __ldg(a.off + v);
+          e0 = __ldg(a.off + v + 1);
         }
-        const unsigned tm = __ballot_sync(kFull, take);
-        if (OP != OP_BFS) {
-          const bool kept = act && !take;
-          const uint32_t kmin = warp_min(kept ? vval : 0xFFFFFFFFu);
-          my_min = min(my_min, kmin);
-          if (lane == 0) {
-            my_keep += __popc(wd & ~tm);
-            a.wmin[wbase + j] = kmin;
-          }
-        }
-        if (lane == 0 && tm) a.bm[wbase + j] = wd & ~tm;
+        const uint32_t vval = in ? ldcg(a.val + v) : 0u;
+        const bool take = in && (OP == OP_BFS || vval < thr);
+        if (take) atomicOr(&s_tk[own], 1u << (v & 31u));
+        else if (OP != OP_BFS && in) atomicMin(&s_km[own], vval);
         uint32_t deg = 0;
         unsigned long long eaddr = 0;
         if (take) {
-          if (OP == OP_BFS) vval = ldcg(a.val + v);
-          const uint64_t s = __ldg(a.off + v), e = __ldg(a.off + v + 1);
-          deg = (uint32_t)(e - s);
+          if (OP != OP_BFS) {
+            s0 = __ldg(a.off + v);
+            e0 = __ldg(a.off + v + 1);
+          }
+          deg = (uint32_t)(e0 - s0);
           bool host;
           const uint32_t bi = find_block(vb, a.nblk, v);
-          eaddr = list_addr(a.lc, bbase[bi], a.host_base, v, s, deg, ESZ, &host);
+          eaddr = list_addr(a.lc, bbase[bi], a.host_base, v, s0, deg, ESZ, &host);
           if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
           my_edges += deg;
           my_verts += 1;
@@ -440,17 +704,33 @@ __global__ void __launch_bounds__(kMinThreads)
           base = shfl64(base, 0);
           if (big) {
             unsigned long long pos = base + inc - nch;
-            for (unsigned k = 0; k < nch; k++, pos++) {
-              const uint32_t lo = k * a.chunk;
-              const uint32_t cnt = min(a.chunk, deg - lo);
+            for (unsigned kk = 0; kk < nch; kk++, pos++) {
+              const uint32_t lo = kk * a.chunk;
+              const uint32_t cn = min(a.chunk, deg - lo);
               if (pos < a.cap_b)
-                a.qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, cnt, v, vval);
+                a.qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, cn, v, vval);
               else
                 atomicCAS(&c->err, 0u, kDevErrQueue);
             }
           }
         }
       }
+      __syncwarp();
+      if (nsub > 1) {
+        unsigned last = 0;
+        if (lane == 0) last = atomicInc(a.wmin + g, nsub - 1u) == nsub - 1u;
+        if (__shfl_sync(kFull, last, 0) && act_word) a.bm[wbase + lane] = 0;
+      } else if (act_word) {
+        const uint32_t tk = s_tk[lane];
+        if (OP != OP_BFS) {
+          const uint32_t km = s_km[lane];
+          a.wmin[wbase + lane] = km;
+          my_keep += __popc(word & ~tk);
+          my_min = min(my_min, km);
+        }
+        if (tk) a.bm[wbase + lane] = word & ~tk;
+      }
+      __syncwarp();
     }
     my_edges = warp_sum(my_edges);
     my_hbm = warp_sum(my_hbm);
@@ -488,43 +768,30 @@ __global__ void __launch_bounds__(kMinThreads)
       thr = (uint32_t)min((unsigned long long)mk + width, 0xFFFFFFFFull);
       continue;
     }
-    if (OP == OP_BFS) {
-      // Direction for this level (the same decision in every thread: it
-      // reads only counters complete at the barrier).  Top-down -> bottom-up
-      // when the frontier's out-edges exceed the unexplored edges / alpha;
-      // back when the frontier holds fewer than nv / beta vertices, or when
-      // its out-edges fall below half the in-edges the last bottom-up level
-      // scanned (the rest are vertices bottom-up keeps rescanning).
-      const unsigned long long mf = ldcg(&c->mf[slot]), nf = ldcg(&c->nf[slot]);
-      mu = mu > mf ? mu - mf : 0;
-      if (a.do_alpha)
-        bottom_up = bottom_up ? nf * a.do_beta >= a.nv && 2 * mf > last_scan
-                              : mf * a.do_alpha > mu;
-      if (!bottom_up) {
-        if (leader) atomicAdd(&c->edges, mf);
-      } else {
-        bfs_bottom_up(a.in_off, a.in_adj, a.bm2, a.bm, a.val, a.nv, iter + 2u, &c->edges,
-                      &c->bu_scan[slot], gwarp, nwarps);
-        if (leader) c->bu_levels++;
-        if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
-        last_scan = ldcg(&c->bu_scan[slot]);
-        continue;
-      }
-    }
+    if (OP == OP_BFS && leader) atomicAdd(&c->edges, ldcg(&c->mf[slot]));
     // ----------------------------------------------------------- expansion
     // task ids: chunks first, then groups of 32 small vertices; each warp
     // starts on task gwarp, then draws from a shared counter (no atomic at
     // all for warps without a first task)
-    const unsigned long long ntask = nb + (ns + 31) / 32;
+    // With fewer tasks than warps, each chunk is split into up to 8 parts
+    // (one task each) so that more warps share a small level's edges,
+    // and groups of small vertices get smaller (down to 4 vertices)
+    unsigned gsize = 32;
+    while (gsize > 4 && nb + (ns + gsize - 1) / gsize < nwarps / 2) gsize >>= 1;
+    const unsigned long long ngrp = (ns + gsize - 1) / gsize;
+    const unsigned parts =
+        nb && nb + ngrp < nwarps ? (unsigned)min(8ull, max(1ull, (nwarps - ngrp) / nb)) : 1u;
+    const unsigned long long nbt = nb * parts;
+    const unsigned long long ntask = nbt + ngrp;
     for (unsigned long long t = gwarp; t < ntask;) {
       // reserve the next task before working on this one (latency overlap)
       unsigned long long nt = 0;
       if (lane == 0) nt = atomicAdd(&c->wc[slot], 1ull);
-      if (t < nb) {
-        const MinItem it = a.qb[t];
-        process_chunk<OP, ESZ>(a, it);
+      if (t < nbt) {
+        const MinItem it = a.qb[t / parts];
+        process_chunk<OP, ESZ>(a, it, (unsigned)(t % parts), parts);
       } else {
-        process_group<OP, ESZ>(a, (t - nb) * 32ull, ns);
+        process_group<OP, ESZ>(a, (t - nbt) * gsize, ns, gsize);
       }
       t = nwarps + shfl64(nt, 0);
     }
@@ -557,6 +824,10 @@ __global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
     }
     a.bm[w] = word;
     if (OP == OP_SSSP) a.wmin[w] = w == (a.src >> 5) ? 1u : 0xFFFFFFFFu;
+    // BFS: per-group counters of the warps that share a compaction group,
+    // and the second frontier bitmap of direction-optimising runs
+    if (OP == OP_BFS && a.wmin) a.wmin[w] = 0;
+    if (OP == OP_BFS && a.bm2) a.bm2[w] = 0;
   }
   if (tid == 0) {
     MinCtrl *c = a.ctrl;
@@ -670,21 +941,6 @@ constexpr int kScanPer = 4;
 // Queue-mode small-vertex groups: edges per lane per step (2 and 4
 // measured slower at RMAT-24).
 constexpr int kGroupPer = 8;
-
-// Position of the n-th (from 0) set bit of x; n < popc(x).
-__device__ __forceinline__ uint32_t nth_set_bit(uint32_t x, uint32_t n) {
-  uint32_t pos = 0;
-#pragma unroll
-  for (uint32_t s = 16; s > 0; s >>= 1) {
-    const uint32_t lo = __popc(x & ((1u << s) - 1u));
-    if (n >= lo) {
-      n -= lo;
-      x >>= s;
-      pos += s;
-    }
-  }
-  return pos;
-}
 
 // Relax N edges per lane; near improvements are queued, far ones parked.
 // Each dependent step (value probe, atomicMin, tag probe, tag atomicMax) is
@@ -1356,7 +1612,8 @@ void minprop_free(thv_graph *g) {
 template <int OP, int ESZ>
 static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
                                  uint32_t &launches, bool scan_mode) {
-  auto kern = scan_mode ? minprop_kernel<OP, ESZ> : minq_kernel<OP, ESZ>;
+  auto kern = scan_mode ? (OP == OP_BFS && a.do_alpha ? bfs_do_kernel<ESZ> : minprop_kernel<OP, ESZ>)
+                        : minq_kernel<OP, ESZ>;
   const size_t nb = g->plan.blocks.size();
   const size_t smem = nb <= kSmemBlocks ? nb * 8 + (nb + 1) * 4 : 0;
   THV_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1569,17 +1826,20 @@ const uint32_t *minprop_device_values(thv_graph *g) {
 // at zero (bitmap, counters) on every call, and calls whose work overlaps
 // on the GPU (concurrent streams, or several host threads) race on it --
 // serialise them.  The first call on a device looks up the array's device
-// address (cudaGetSymbolAddress); make that first call before any stream
-// capture.
+// address (cudaGetSymbolAddress) and the device's SM count; make that first
+// call before any stream capture.  The address is kept for the life of the
+// process, so a cudaDeviceReset after the first call is not supported.
 namespace thv {
 
 constexpr size_t kNoAllocScratchBytes = 64ull << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 // Host code may not take the array's address directly (a host-side shadow,
-// not a device address): this is the looked-up device address per device.
+// not a device address): this is the looked-up device address per device,
+// with that device's SM count.
 static std::mutex g_noalloc_mu;
 static uintptr_t g_noalloc_addr[64];
+static int g_noalloc_sms[64];
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
@@ -1613,7 +1873,7 @@ __global__ void noalloc_table_init(uint32_t *vb, uint64_t *base, uint32_t nv, ui
   base[0] = adj;
 }
 
-static thv_status noalloc_scratch_address(int dev, uintptr_t *addr) {
+static thv_status noalloc_scratch_address(int dev, uintptr_t *addr, int *sms) {
   if (dev < 0 || dev >= 64) return fail(THV_EUNSUPPORTED, "device %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_noalloc_mu);
   if (!g_noalloc_addr[dev]) {
@@ -1621,9 +1881,13 @@ static thv_status noalloc_scratch_address(int dev, uintptr_t *addr) {
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p)
       return fail(THV_ECUDA, "cudaGetSymbolAddress(no-alloc scratch): %s", cudaGetErrorString(e));
+    int n = 0;
+    THV_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    g_noalloc_sms[dev] = n;
     g_noalloc_addr[dev] = (uintptr_t)p;
   }
   *addr = g_noalloc_addr[dev];
+  *sms = g_noalloc_sms[dev];
   return THV_OK;
 }
 
@@ -1646,9 +1910,8 @@ static thv_status bfs_noalloc(const uint64_t *d_off, const uint32_t *d_adj, uint
   int dev = 0;
   THV_CUDA(cudaGetDevice(&dev));
   uintptr_t base = 0;
-  THV_TRY(noalloc_scratch_address(dev, &base));
-  cudaDeviceProp prop;
-  THV_CUDA(cudaGetDeviceProperties(&prop, dev));
+  int sms = 0;
+  THV_TRY(noalloc_scratch_address(dev, &base, &sms));
 
   MinArgs a{};
   a.val = d_values;
@@ -1677,16 +1940,20 @@ static thv_status bfs_noalloc(const uint64_t *d_off, const uint32_t *d_adj, uint
 
   noalloc_table_init<<<1, 1, 0, st>>>((uint32_t *)a.blk_vb, (uint64_t *)a.blk_base, (uint32_t)nv,
                                       (uint64_t)(uintptr_t)d_adj);
-  const int init_grid = std::max(1, std::min<int>(prop.multiProcessorCount * 8, (int)((nv + 255) / 256)));
+  const int init_grid = std::max(1, std::min<int>(sms * 8, (int)((nv + 255) / 256)));
   minprop_init<OP_BFS><<<init_grid, 256, 0, st>>>(a, l.ngroups * 32u);
   THV_CUDA(cudaGetLastError());
   auto kern = minprop_kernel<OP_BFS, 4>;
   const size_t smem = 1 * 8 + 2 * 4;
+  // thv_run sets this kernel's dynamic shared memory limit per plan (down
+  // to 0 for large block tables); this launch needs its own
+  THV_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem));
   int bpsm = 0;
   THV_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, kern, kMinThreads, smem));
   if (bpsm < 1) return fail(THV_ECUDA, "BFS kernel cannot be resident");
   void *args[] = {&a};
-  THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(bpsm * prop.multiProcessorCount),
+  THV_CUDA(cudaLaunchCooperativeKernel((void *)kern, dim3(bpsm * sms),
                                        dim3(kMinThreads), args, smem, st));
   MinCtrl hc;  // the caller's stack: nothing allocated
   THV_CUDA(cudaMemcpyAsync(&hc, a.ctrl, sizeof(MinCtrl), cudaMemcpyDeviceToHost, st));

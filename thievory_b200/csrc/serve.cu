@@ -490,6 +490,13 @@ constexpr uint64_t kGroupBytesPerVertex = 600;
 // (1.16x; 3: 0.91x), of k SSSP sources from k = 6 (1.17x; 4: 0.90x).
 constexpr uint32_t kGroupMinBfs = 4, kGroupMinSssp = 6;
 constexpr uint32_t kGroupMax = 64;
+// Iterations a running group admits arrivals.  RMAT-26 edge factor 48, 256
+// queries (80% BFS), Poisson arrivals at 32x the single-run capacity:
+// admitting for a group's whole life 61.8 q/s (p99 3.3 s), for its first 2
+// iterations 98.2 q/s (p99 1.9 s), only at its start 85.1 q/s; at 4x the
+// capacity p50 2.3 s / 0.93 s / 0.91 s.  Sources that start more than a
+// level or two apart share few edge reads.
+constexpr uint32_t kJoinWindow = 2;
 
 }  // namespace
 
@@ -499,6 +506,7 @@ struct thv_server {
   bool batching = true;    // batched groups + lone runs (false: slots)
   uint32_t group_min = 0;  // explicit group threshold; 0 = per algorithm
   uint32_t replan_every = 0;        // queries between access re-placements
+  uint32_t join_window = 0;         // iterations a running group admits arrivals; 0 = always
   uint64_t done_since_replan = 0;
   uint64_t timeout_ns = 0;
   // device state
@@ -524,12 +532,18 @@ struct thv_server {
   thv_status fatal = THV_OK;
   std::string fatal_msg;
   std::thread worker;
-  // batching: one live group per algorithm (BFS, SSSP) and the ticket and
-  // start iteration of each mask bit
-  LiveGroup live[2];
-  bool live_open[2] = {false, false};
-  uint64_t live_ticket[2][64] = {};
-  uint32_t live_iter0[2][64] = {};
+  // batching: up to kLiveGroups live groups per algorithm (BFS, SSSP), and
+  // the ticket and start iteration of each mask bit
+  LiveGroup live[2][2];
+  bool live_open[2][2] = {};
+  uint64_t live_ticket[2][2][64] = {};
+  uint32_t live_iter0[2][2][64] = {};
+  // Groups of one algorithm on the device at once.  A second group (for the
+  // arrivals after the first one's join window) measured slower at
+  // RMAT-26 edge factor 48: 72.9 against 90.2 q/s at 32x the single-run
+  // capacity, p50 1.41 against 0.96 s at 4x: turns between two groups delay
+  // both.
+  uint32_t groups_per_algo = 1;
 };
 
 namespace {
@@ -541,7 +555,8 @@ double clock_ms() {
 
 void server_free(thv_server *s) {
   for (int k = 0; k < 2; k++)
-    if (s->live_open[k]) live_close(&s->live[k]);
+    for (int i = 0; i < 2; i++)
+      if (s->live_open[k][i]) live_close(&s->live[k][i]);
   dev_free(s->d_val);
   dev_free(s->d_bm);
   dev_free(s->d_out);
@@ -678,35 +693,37 @@ void fail_all(thv_server *s, thv_status st, const std::string &msg) {
 // returns to the host).
 constexpr uint32_t kLiveItersBusy = 1;
 
-// Adds tickets (all of algorithm k) to live group k, opening it on first use.
-thv_status live_join(thv_server *s, int k, const std::vector<uint64_t> &tickets) {
+// Adds tickets (all of algorithm k) to live group (k, i), opening it on
+// first use.
+thv_status live_join(thv_server *s, int k, int i, const std::vector<uint64_t> &tickets) {
   if (tickets.empty()) return THV_OK;
   thv_graph *g = s->g;
-  if (!s->live_open[k]) {
-    THV_TRY(live_open(g, &s->live[k], k == 1));
-    s->live_open[k] = true;
+  LiveGroup &lg = s->live[k][i];
+  if (!s->live_open[k][i]) {
+    s->live_open[k][i] = true;  // live_close frees whatever live_open allocated
+    THV_TRY(live_open(g, &lg, k == 1));
   }
   std::vector<uint32_t> src(tickets.size()), bits(tickets.size());
   {
     std::lock_guard<std::mutex> lk(s->mu);
-    for (size_t i = 0; i < tickets.size(); i++) src[i] = s->queries[tickets[i]].source;
+    for (size_t j = 0; j < tickets.size(); j++) src[j] = s->queries[tickets[j]].source;
   }
-  THV_TRY(live_add(g, &s->live[k], (uint32_t)src.size(), src.data(), bits.data(),
+  THV_TRY(live_add(g, &lg, (uint32_t)src.size(), src.data(), bits.data(),
                    (uint32_t)(s->timeout_ns / 1000000ull), s->st));
   std::lock_guard<std::mutex> lk(s->mu);
-  for (size_t i = 0; i < tickets.size(); i++) {
-    s->live_ticket[k][bits[i]] = tickets[i];
-    s->live_iter0[k][bits[i]] = s->live[k].iter;
-    s->queries[tickets[i]].slot = bits[i];
+  for (size_t j = 0; j < tickets.size(); j++) {
+    s->live_ticket[k][i][bits[j]] = tickets[j];
+    s->live_iter0[k][i][bits[j]] = lg.iter;
+    s->queries[tickets[j]].slot = bits[j];
   }
   return THV_OK;
 }
 
 thv_status run_alone(thv_server *s, thv_algo algo, uint64_t ticket);
 
-// One launch of live group k, then its finished sources' results.
-thv_status live_turn(thv_server *s, int k, uint32_t iters) {
-  LiveGroup &lg = s->live[k];
+// One launch of live group (k, i), then its finished sources' results.
+thv_status live_turn(thv_server *s, int k, int i, uint32_t iters) {
+  LiveGroup &lg = s->live[k][i];
   unsigned long long fin = 0;
   bool too_deep = false;
   const uint32_t tmo = (uint32_t)(s->timeout_ns / 1000000ull);
@@ -714,7 +731,7 @@ thv_status live_turn(thv_server *s, int k, uint32_t iters) {
   if (too_deep) {
     // a BFS level left the u8 range: its queries run alone instead
     std::vector<uint64_t> redo;
-    for (unsigned long long m = lg.active; m; m &= m - 1) redo.push_back(s->live_ticket[k][__builtin_ctzll(m)]);
+    for (unsigned long long m = lg.active; m; m &= m - 1) redo.push_back(s->live_ticket[k][i][__builtin_ctzll(m)]);
     lg.active = 0;
     lg.running = false;
     {
@@ -731,7 +748,7 @@ thv_status live_turn(thv_server *s, int k, uint32_t iters) {
     std::lock_guard<std::mutex> lk(s->mu);
     for (unsigned long long m = fin; m; m &= m - 1) {
       const int b = __builtin_ctzll(m);
-      outs[b] = s->queries[s->live_ticket[k][b]].out;
+      outs[b] = s->queries[s->live_ticket[k][i][b]].out;
     }
   }
   THV_TRY(live_collect(s->g, &lg, fin, sums, outs, s->d_out, s->st));
@@ -739,13 +756,13 @@ thv_status live_turn(thv_server *s, int k, uint32_t iters) {
   const double now = clock_ms();
   for (unsigned long long m = fin; m; m &= m - 1) {
     const int b = __builtin_ctzll(m);
-    Query &q = s->queries[s->live_ticket[k][b]];
+    Query &q = s->queries[s->live_ticket[k][i][b]];
     q.checksum = sums[b];
     q.t_done = now;
-    q.iterations = lg.iter - s->live_iter0[k][b];
+    q.iterations = lg.iter - s->live_iter0[k][i][b];
     q.status = THV_OK;
     q.done = true;
-    s->live_ticket[k][b] = 0;
+    s->live_ticket[k][i][b] = 0;
     s->done_since_replan++;
   }
   s->cv_done.notify_all();
@@ -783,15 +800,23 @@ thv_status run_alone(thv_server *s, thv_algo algo, uint64_t ticket) {
   return st;
 }
 
-bool live_running(const thv_server *s) { return s->live[0].running || s->live[1].running; }
+bool live_running(const thv_server *s, int k) {
+  return s->live[k][0].running || s->live[k][1].running;
+}
+bool live_running(const thv_server *s) { return live_running(s, 0) || live_running(s, 1); }
 
-// Batching mode, one dispatcher round: admit waiting queries into the live
-// groups (a running group takes them into free mask bits; a group that is
-// not running starts when enough of its algorithm wait, or at once when the
-// other algorithm's group is on the device), run a lone query when nothing
-// is live and too few wait, then give each running group one turn.
+// Batching mode, one dispatcher round.  Admission, per algorithm: a running
+// group still inside its join window (its first join_window iterations)
+// takes waiting queries into free mask bits -- sources that start within a
+// couple of levels of each other share most edge reads; otherwise a new
+// group starts when enough queries wait (group_min), or at once when no
+// group of this algorithm runs but the other algorithm's does (they share
+// the device by turns anyway), up to groups_per_algo groups, so arrivals
+// need not wait for an old group to drain.  With nothing on the device and
+// too few waiting, the front query runs alone.  Then every running group
+// gets one turn.
 thv_status batching_round(thv_server *s) {
-  std::vector<uint64_t> joins[2];
+  std::vector<uint64_t> joins[2][2];
   uint64_t alone = 0;
   thv_algo alone_algo = THV_ALGO_BFS;
   bool waiting_for[2] = {false, false};
@@ -803,17 +828,32 @@ thv_status batching_round(thv_server *s) {
       uint32_t n = 0;
       for (uint64_t t : s->waiting) n += s->queries[t].algo == algo;
       if (!n) continue;
-      LiveGroup &lg = s->live[k];
-      const bool running = lg.running;
+      int inst = -1;
       uint32_t take = 0;
-      if (running) {
-        if (live_can_join(s->g, &lg)) take = std::min<uint32_t>(n, kGroupMax - __builtin_popcountll(lg.active));
-      } else {
+      bool joined = false;
+      for (int i = 0; i < (int)s->groups_per_algo && inst < 0; i++) {
+        LiveGroup &lg = s->live[k][i];
+        if (lg.running && live_can_join(s->g, &lg) && (!s->join_window || lg.iter < s->join_window)) {
+          inst = i;
+          take = std::min<uint32_t>(n, kGroupMax - __builtin_popcountll(lg.active));
+          joined = true;
+        }
+      }
+      if (inst < 0) {
         const uint32_t kmin = s->group_min ? s->group_min : (k ? kGroupMinSssp : kGroupMinBfs);
-        if (n >= kmin || s->live[1 - k].running) take = std::min<uint32_t>(n, kGroupMax);
+        const bool any_k = live_running(s, k);
+        for (int i = 0; i < (int)s->groups_per_algo && inst < 0; i++) {
+          if (s->live[k][i].running) continue;
+          if (n >= kmin || (!any_k && live_running(s, 1 - k))) {
+            inst = i;
+            take = std::min<uint32_t>(n, kGroupMax);
+          }
+        }
       }
       waiting_for[k] = take < n;
-      for (auto it = s->waiting.begin(); it != s->waiting.end() && joins[k].size() < take;) {
+      if (inst < 0) continue;
+      std::vector<uint64_t> &jv = joins[k][inst];
+      for (auto it = s->waiting.begin(); it != s->waiting.end() && jv.size() < take;) {
         Query &q = s->queries[*it];
         if (q.algo != algo) {
           ++it;
@@ -821,12 +861,15 @@ thv_status batching_round(thv_server *s) {
         }
         q.t_start = now;
         q.mode = 1;
-        q.joined = running;
-        joins[k].push_back(*it);
+        q.joined = joined;
+        jv.push_back(*it);
         it = s->waiting.erase(it);
       }
     }
-    if (joins[0].empty() && joins[1].empty() && !live_running(s) && !s->waiting.empty()) {
+    bool any_join = false;
+    for (int k = 0; k < 2; k++)
+      for (int i = 0; i < 2; i++) any_join |= !joins[k][i].empty();
+    if (!any_join && !live_running(s) && !s->waiting.empty()) {
       alone = s->waiting.front();
       s->waiting.pop_front();
       Query &q = s->queries[alone];
@@ -836,17 +879,22 @@ thv_status batching_round(thv_server *s) {
     }
   }
   if (alone) return run_alone(s, alone_algo, alone);
-  for (int k = 0; k < 2; k++) THV_TRY(live_join(s, k, joins[k]));
-  const bool both = s->live[0].running && s->live[1].running;
+  for (int k = 0; k < 2; k++)
+    for (int i = 0; i < 2; i++) THV_TRY(live_join(s, k, i, joins[k][i]));
+  int nrunning = 0;
+  for (int k = 0; k < 2; k++)
+    for (int i = 0; i < 2; i++) nrunning += s->live[k][i].running;
   for (int k = 0; k < 2; k++) {
-    if (!s->live[k].running) continue;
-    bool waits;
-    {
-      std::lock_guard<std::mutex> lk(s->mu);
-      waits = !s->waiting.empty();
+    for (int i = 0; i < 2; i++) {
+      if (!s->live[k][i].running) continue;
+      bool waits;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        waits = !s->waiting.empty();
+      }
+      const uint32_t iters = nrunning > 1 || waits || waiting_for[k] ? kLiveItersBusy : s->batch_iters;
+      THV_TRY(live_turn(s, k, i, iters));
     }
-    const uint32_t iters = both || waits || waiting_for[k] ? kLiveItersBusy : s->batch_iters;
-    THV_TRY(live_turn(s, k, iters));
   }
   return THV_OK;
 }
@@ -981,6 +1029,9 @@ thv_status start(thv_graph *g, const thv_serve_opts *o, thv_server **out) {
   s->batching = !(o && o->group_min == 0xFFFFFFFFu);
   s->group_min = o && o->group_min && o->group_min != 0xFFFFFFFFu ? o->group_min : 0u;
   s->replan_every = o ? o->replan_every : 0;
+  s->join_window = o && o->join_window ? (o->join_window == 0xFFFFFFFFu ? 0u : o->join_window)
+                                       : kJoinWindow;
+  s->groups_per_algo = o && o->groups_per_algo ? std::min<uint32_t>(o->groups_per_algo, 2u) : 1u;
   if (o && o->mem_budget_bytes && o->mem_budget_bytes < g->nv * kGroupBytesPerVertex)
     s->batching = false;  // the batch state does not fit the memory budget
   s->timeout_ns = (uint64_t)(o && o->timeout_ms ? o->timeout_ms : 60000u) * 1000000ull;

@@ -210,6 +210,7 @@ struct LiveGroup {
   uint32_t *d_buf = nullptr, *h_buf = nullptr;       // 4 x 64 u32 staging
   unsigned long long *d_sums = nullptr, *h_sums = nullptr;
   uint64_t edges = 0, hbm_bytes = 0, link_bytes = 0;  // since the group started
+  BatchState *bs = nullptr;  // the group's own traversal state
 };
 thv_status live_open(thv_graph *g, LiveGroup *lg, bool sssp);
 void live_close(LiveGroup *lg);
