@@ -110,9 +110,10 @@ struct MinArgs {
   MinItem *qs, *qb;
   unsigned long long cap_s, cap_b;
   MinCtrl *ctrl;
-  // queue mode: second queue buffers and the per-vertex queue tags
+  // queue mode: second queue buffers and two queued-vertex bitmaps (one
+  // per phase parity, ngroups * 32 words each)
   MinItem *qs2, *qb2;
-  uint32_t *qtag;
+  uint32_t *qbits;
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, max_iters;
   uint32_t delta, small_deg, chunk, src;
@@ -136,7 +137,7 @@ struct MinState {
   uint32_t *d_bm2 = nullptr;  // BFS frontier copy for bottom-up levels
   MinItem *d_qs = nullptr, *d_qb = nullptr;
   MinItem *d_qs2 = nullptr, *d_qb2 = nullptr;
-  uint32_t *d_qtag = nullptr;
+  uint32_t *d_qbits = nullptr;
   uint64_t cap_s = 0, cap_b = 0;
   uint32_t chunk = 0, small = 0;
   MinCtrl *d_ctrl = nullptr;
@@ -845,17 +846,22 @@ __global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
 // The bitmap scan runs only when the near queue is empty: at the start, and
 // when an SSSP/CC window advances over vertices parked in the far bitmap.
 //
-// SSSP/CC push a vertex at most once per queue through a per-vertex tag:
-// phase ph appends to its output queue with tag ph + 1, and a relaxation that
-// lowers w below the window pushes it only if atomicMax(tag[w], ph + 1) saw a
-// smaller tag.  Invariant: tag[w] == ph + 1 implies w has an entry in phase
-// ph's output queue, which the next phase expands after a grid barrier and
-// so with the final value of this phase.  The expander of phase ph therefore
-// skips an entry whose tag already reads ph + 1 (it is queued again, with a
-// lower value); otherwise it expands with the value it reads.  No decrease is
-// lost under any ordering of the two sides, so no fence is needed; a late
-// tag read only costs a redundant expansion.  BFS needs no tags: a vertex
-// changes once and its pusher is unique.
+// SSSP/CC push a vertex at most once per queue through two bitmaps of
+// queued vertices, one per phase parity (one bit per vertex: small enough
+// to stay in L2 beside the values, which per-vertex 4-byte tags were not).
+// A relaxation in phase ph that lowers w below the window pushes it only if
+// its atomicOr on w's bit in Q[ph & 1] found the bit clear.  Invariant: w's
+// bit in Q[ph & 1] set implies w has an entry in phase ph's output queue,
+// which phase ph + 1 expands after a grid barrier and so with the final
+// value of phase ph.  The expander of phase ph + 1 clears the bit of every
+// entry it takes in Q[ph & 1] (so Q[ph & 1] is empty again when phase ph + 2
+// pushes into it) and skips an entry whose bit in Q[(ph + 1) & 1] is already
+// set (it is queued again, with a lower value); otherwise it expands with
+// the value it reads.  No decrease is lost under any ordering of the two
+// sides, so no fence is needed; a late bit read only costs a redundant
+// expansion.  Entries queued by a bitmap scan have no bit (the scan takes
+// each vertex once).  BFS needs neither: a vertex changes once and its
+// pusher is unique.
 
 struct QStats {
   unsigned long long edges = 0, hbm = 0, link = 0;
@@ -930,7 +936,8 @@ struct QEnv {
   MinItem *qs_next, *qb_next;
   unsigned cs_next;
   uint32_t thr;
-  uint32_t tag;  // tag of the output queue: phase + 1
+  uint32_t *qnext;  // queued bits of this phase's output queue
+  uint32_t *qprev;  // queued bits of the queue this phase expands
   uint2 *stage;  // this warp's shared list of vertices to queue: (w, value)
 };
 
@@ -954,11 +961,14 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
                                           const uint32_t (&cand)[N], const bool (&ok)[N],
                                           QStats &qst) {
   static_assert(N <= kQRelaxMax, "staging list holds kQRelaxMax entries per lane");
+  // values stay in L2 (evict-last) while edges and items stream through
+  const unsigned long long keep = l2_evict_last();
   uint32_t r[N];
 #pragma unroll
-  for (int j = 0; j < N; j++) r[j] = ok[j] ? ldcg(a.val + w[j]) : 0u;
+  for (int j = 0; j < N; j++) r[j] = ok[j] ? ldcg_hint(a.val + w[j], keep) : 0u;
 #pragma unroll
-  for (int j = 0; j < N; j++) r[j] = ok[j] && cand[j] < r[j] ? atomicMin(a.val + w[j], cand[j]) : 0u;
+  for (int j = 0; j < N; j++)
+    r[j] = ok[j] && cand[j] < r[j] ? atomic_min_hint(a.val + w[j], cand[j], keep) : 0u;
   bool push[N];
 #pragma unroll
   for (int j = 0; j < N; j++) {
@@ -972,12 +982,16 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
     }
   }
   if (OP != OP_BFS) {
+    // push only if w's queued bit was clear: probe it, then claim it
 #pragma unroll
-    for (int j = 0; j < N; j++) r[j] = push[j] ? ldcg(a.qtag + w[j]) : e.tag;
+    for (int j = 0; j < N; j++) r[j] = push[j] ? ldcg(e.qnext + (w[j] >> 5)) : 0xFFFFFFFFu;
 #pragma unroll
-    for (int j = 0; j < N; j++) r[j] = r[j] != e.tag ? atomicMax(a.qtag + w[j], e.tag) : e.tag;
+    for (int j = 0; j < N; j++) {
+      const uint32_t m = 1u << (w[j] & 31u);
+      r[j] = (r[j] & m) ? r[j] : atomicOr(e.qnext + (w[j] >> 5), m);
+    }
 #pragma unroll
-    for (int j = 0; j < N; j++) push[j] = push[j] && r[j] < e.tag;
+    for (int j = 0; j < N; j++) push[j] = push[j] && !((r[j] >> (w[j] & 31u)) & 1u);
   }
   const unsigned lane = lane_id();
   unsigned n = 0;
@@ -998,8 +1012,9 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
 }
 
 // Dequeue: BFS values are final when queued.  SSSP/CC clear the vertex's
-// parked bit (its pending value is handled here), read the latest value and
-// report a skip when the vertex is already queued again for the next phase.
+// parked bit (its pending value is handled here) and its queued bit of this
+// queue, read the latest value and report a skip when the vertex is already
+// queued again for the next phase.
 template <int OP>
 __device__ __forceinline__ uint32_t q_dequeue(const MinArgs &a, const QEnv &e, uint32_t v,
                                               uint32_t item_val, bool &skip) {
@@ -1007,8 +1022,9 @@ __device__ __forceinline__ uint32_t q_dequeue(const MinArgs &a, const QEnv &e, u
   if (OP == OP_BFS) return item_val;
   const uint32_t m = 1u << (v & 31u);
   if (ldcg(a.bm + (v >> 5)) & m) atomicAnd(a.bm + (v >> 5), ~m);
-  const uint32_t cur = ldcg(a.val + v);
-  skip = ldcg(a.qtag + v) == e.tag;
+  atomicAnd(e.qprev + (v >> 5), ~m);
+  const uint32_t cur = ldcg_hint(a.val + v, l2_evict_last());
+  skip = (ldcg(e.qnext + (v >> 5)) & m) != 0;
   return cur;
 }
 
@@ -1028,12 +1044,22 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
   const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
   if (lane == 0) q_count(a, qst, start, (unsigned)(it.ea_cnt >> 48), ESZ);
   // two 16-byte loads per lane in flight (1 KiB per warp step): host-link
-  // reads are latency-bound per warp
-  for (uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane; __any_sync(kFull, p < end); p += 1024u) {
-    uint4 q[2];
+  // reads are latency-bound per warp.  The next step's loads are issued
+  // before this step's relaxation, so they travel while its probes and
+  // atomics do.
+  // edges are read once: evict-first
+  const unsigned long long stream = l2_evict_first();
+  uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane;
+  uint4 qn[2];
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+    qn[h] = p + 512u * h < end ? ld_stream_v4(p + 512u * h, stream) : make_uint4(0, 0, 0, 0);
+  for (; __any_sync(kFull, p < end); p += 1024u) {
+    uint4 q[2] = {qn[0], qn[1]};
 #pragma unroll
     for (int h = 0; h < 2; h++)
-      q[h] = p + 512u * h < end ? ld_nc_v4(p + 512u * h) : make_uint4(0, 0, 0, 0);
+      qn[h] = p + 1024u + 512u * h < end ? ld_stream_v4(p + 1024u + 512u * h, stream)
+                                          : make_uint4(0, 0, 0, 0);
     uint32_t w[2 * PER], cand[2 * PER];
     bool ok[2 * PER];
 #pragma unroll
@@ -1087,11 +1113,11 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
       if (ok[h]) {
         const uintptr_t addr = (uintptr_t)ea + (uintptr_t)(t - oex) * ESZ;
         if (ESZ == 4) {
-          const uint32_t ed = ld_nc_u32(addr);
+          const uint32_t ed = ld_stream_u32(addr, l2_evict_first());
           w[h] = edge_dst(ed, a.wshift);
           wt = edge_wt(ed, a.wshift, a.wbase);
         } else {
-          const uint2 ed = ld_nc_u2(addr);
+          const uint2 ed = ld_stream_u2(addr, l2_evict_first());
           w[h] = ed.x;
           wt = ed.y;
         }
@@ -1157,7 +1183,8 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
     env.qb_next = qb_out;
     env.cs_next = cur;
     env.thr = thr;
-    env.tag = ph + 1;
+    env.qnext = a.qbits + (size_t)(ph & 1u) * a.ngroups * 32u;
+    env.qprev = a.qbits + (size_t)((ph + 1u) & 1u) * a.ngroups * 32u;
     if (scan) {
       // ------------------------------------------------------------- scan
       // A warp owns 32 bitmap words (lane = word).  The pending vertices of
@@ -1280,9 +1307,9 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
   if (leader) c->iters = iter;
 }
 
-__global__ void minq_clear(uint32_t *qtag, uint32_t nv) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x)
-    qtag[v] = 0;
+__global__ void minq_clear(uint32_t *qbits, uint32_t nwords) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nwords; i += gridDim.x * blockDim.x)
+    qbits[i] = 0;
 }
 
 __global__ void values_checksum_kernel(const uint32_t *val, uint64_t nv,
@@ -1580,7 +1607,7 @@ static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
   THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(MinItem), "chunk queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qs2, ms->cap_s * sizeof(MinItem), "queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qb2, ms->cap_b * sizeof(MinItem), "chunk queue"));
-  THV_TRY(dev_alloc((void **)&ms->d_qtag, g->nv * 4 + 64, "queue tags"));
+  THV_TRY(dev_alloc((void **)&ms->d_qbits, nw_alloc * 2 * 4, "queued-vertex bitmaps"));
   THV_TRY(dev_alloc((void **)&ms->d_ctrl, sizeof(MinCtrl), "control"));
   THV_TRY(pinned_alloc((void **)&ms->h_ctrl, sizeof(MinCtrl), "control"));
   THV_CUDA(cudaEventCreate(&ms->ev0));
@@ -1600,7 +1627,7 @@ void minprop_free(thv_graph *g) {
   dev_free(ms->d_qb);
   dev_free(ms->d_qs2);
   dev_free(ms->d_qb2);
-  dev_free(ms->d_qtag);
+  dev_free(ms->d_qbits);
   dev_free(ms->d_ctrl);
   pinned_free(ms->h_ctrl);
   if (ms->ev0) cudaEventDestroy(ms->ev0);
@@ -1627,7 +1654,7 @@ static thv_status launch_minprop(thv_graph *g, MinArgs &a, cudaStream_t st,
                                 (int)((g->nv + 255) / 256)));
   minprop_init<OP><<<init_grid, 256, 0, st>>>(a, nw_alloc);
   if (!scan_mode && OP != OP_BFS) {
-    minq_clear<<<init_grid, 256, 0, st>>>(a.qtag, a.nv);
+    minq_clear<<<init_grid, 256, 0, st>>>(a.qbits, a.ngroups * 64u);
     launches++;
   }
   THV_CUDA(cudaGetLastError());
@@ -1688,7 +1715,7 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.qb = ms->d_qb;
   a.qs2 = ms->d_qs2;
   a.qb2 = ms->d_qb2;
-  a.qtag = ms->d_qtag;
+  a.qbits = ms->d_qbits;
   a.cap_s = ms->cap_s;
   a.cap_b = ms->cap_b;
   a.ctrl = ms->d_ctrl;

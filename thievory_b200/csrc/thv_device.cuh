@@ -37,6 +37,57 @@ __device__ __forceinline__ uint2 ld_nc_u2(uintptr_t addr) {
   return __ldg(reinterpret_cast<const uint2 *>(addr));
 }
 
+// L2 eviction priorities (createpolicy + .L2::cache_hint): streaming data
+// read once (edges, queue items) is marked evict-first so that it does not
+// push the randomly probed per-vertex values out of L2; those are marked
+// evict-last.  A hint only orders evictions; results do not depend on it.
+__device__ __forceinline__ unsigned long long l2_evict_first() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ unsigned long long l2_evict_last() {
+  unsigned long long p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// Read-only 16 / 4 / 8-byte streaming loads with an L2 policy, not kept in L1.
+__device__ __forceinline__ uint4 ld_stream_v4(uintptr_t addr, unsigned long long pol) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(addr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_stream_u32(uintptr_t addr, unsigned long long pol) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;"
+               : "=r"(v)
+               : "l"(addr), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint2 ld_stream_u2(uintptr_t addr, unsigned long long pol) {
+  uint2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+               : "=r"(v.x), "=r"(v.y)
+               : "l"(addr), "l"(pol));
+  return v;
+}
+// L2-coherent load / atomic min of a value other SMs write, with an L2 policy.
+__device__ __forceinline__ uint32_t ldcg_hint(const uint32_t *p, unsigned long long pol) {
+  uint32_t v;
+  asm volatile("ld.global.cg.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t atomic_min_hint(uint32_t *p, uint32_t x, unsigned long long pol) {
+  uint32_t old;
+  asm volatile("atom.global.min.L2::cache_hint.u32 %0, [%1], %2, %3;"
+               : "=r"(old)
+               : "l"(p), "r"(x), "l"(pol)
+               : "memory");
+  return old;
+}
+
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
