@@ -975,21 +975,16 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
     const bool imp = cand[j] < r[j];  // 0 when not attempted
     push[j] = imp && (OP == OP_BFS || cand[j] < e.thr);
     if (OP != OP_BFS && imp && !push[j]) {
+      // parked: fire-and-forget updates (nothing waits on them)
       atomicMin(a.wmin + (w[j] >> 5), cand[j]);
-      const uint32_t m = 1u << (w[j] & 31u);
-      uint32_t *bp = a.bm + (w[j] >> 5);
-      if (!(ldcg(bp) & m)) atomicOr(bp, m);
+      atomicOr(a.bm + (w[j] >> 5), 1u << (w[j] & 31u));
     }
   }
   if (OP != OP_BFS) {
-    // push only if w's queued bit was clear: probe it, then claim it
+    // push only if w's queued bit was clear: claim it
 #pragma unroll
-    for (int j = 0; j < N; j++) r[j] = push[j] ? ldcg(e.qnext + (w[j] >> 5)) : 0xFFFFFFFFu;
-#pragma unroll
-    for (int j = 0; j < N; j++) {
-      const uint32_t m = 1u << (w[j] & 31u);
-      r[j] = (r[j] & m) ? r[j] : atomicOr(e.qnext + (w[j] >> 5), m);
-    }
+    for (int j = 0; j < N; j++)
+      r[j] = push[j] ? atomicOr(e.qnext + (w[j] >> 5), 1u << (w[j] & 31u)) : 0xFFFFFFFFu;
 #pragma unroll
     for (int j = 0; j < N; j++) push[j] = push[j] && !((r[j] >> (w[j] & 31u)) & 1u);
   }
