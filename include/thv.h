@@ -26,7 +26,7 @@
  *                               CSR<E>::DumpValues     src/graph.cuh:817-852
  *   thv_save                    converter/converter.cpp:483-589 (.csc),
  *                               :676-774 (.csr), :775-805 (.wcsr)
- *   thv_batch_run, thv_serve_*, thv_generate_rmat
+ *   thv_batch_run, thv_batch_tuned, thv_serve_*, thv_generate_rmat
  *                               no counterpart in the reference (new surface)
  */
 #ifndef THV_H
@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define THV_ABI_VERSION 3
+#define THV_ABI_VERSION 4
 
 typedef enum thv_status {
   THV_OK = 0,
@@ -275,7 +275,31 @@ typedef struct thv_batch_opts {
                             graph shape in memory and in $THV_TUNE_CACHE or
                             ~/.cache/thievory_b200_batch_tune.txt) */
   uint32_t sssp_growth;  /* SSSP window width factor per advance; 0 = default */
+  /* Degree buckets of the expansion.  Vertices of out-degree below
+   * small_degree go in groups of small_group per warp, those below
+   * mid_degree in groups of mid_group per warp (a group's warp spreads the
+   * group's edges over its 32 lanes), the rest in chunks of chunk_edges
+   * edges per warp.  Any of small_degree, chunk_edges, mid_degree,
+   * small_group, mid_group non-zero selects an explicit configuration (the
+   * zeros among them take the defaults: mid_degree = small_degree, i.e. no
+   * middle bucket; small_group 32; mid_group 4); all zero selects the tuned
+   * or default one. */
+  uint32_t mid_degree;
+  uint32_t small_group;  /* 1..32 */
+  uint32_t mid_group;    /* 1..32 */
+  uint32_t pad;
 } thv_batch_opts;
+
+/* The batch kernel's launch configuration for a graph and algorithm: the
+ * autotuned one when thv_batch_run with tune = 1 has timed it for a graph of
+ * this shape (tuned = 1), else the default (tuned = 0). */
+typedef struct thv_batch_config {
+  uint32_t small_degree, mid_degree, chunk_edges, threads;
+  uint32_t small_group, mid_group;
+  uint32_t tuned, pad;
+} thv_batch_config;
+
+thv_status thv_batch_tuned(thv_graph *g, thv_algo algo, thv_batch_config *out);
 
 /* Runs n sources in groups sharing one traversal each.  out (host, may be
  * NULL): n x nv u32, row i = values for sources[i] in the single-source

@@ -24,7 +24,7 @@ def test_library_exports_every_declared_symbol(T, root):
 
 def test_version_and_status_strings(T):
     lib = T.load_library()
-    assert lib.thv_abi_version() == 3
+    assert lib.thv_abi_version() == 4
     assert lib.thv_status_str(0) == b"ok"
     assert lib.thv_status_str(3) == b"malformed graph file"
 

@@ -138,8 +138,12 @@ def test_autotuner_picks_and_caches_a_configuration(T, O, g14, tmp_path, monkeyp
         for i, s in enumerate(src):
             assert np.array_equal(out[i], O.bfs(g14, int(s)))
         line = cache.read_text().strip().splitlines()[-1]
-        small, chunk, threads = map(int, line.split("|")[1].split())
+        small, chunk, threads, mid, gsmall, gmid = map(int, line.split("|")[1].split())
         assert threads in (256, 512) and small >= 16 and chunk >= 128
+        assert mid >= small and 1 <= gsmall <= 32 and 1 <= gmid <= 32
+        assert g.batch_tuned("bfs") == {"small_degree": small, "mid_degree": mid,
+                                        "chunk_edges": chunk, "threads": threads,
+                                        "small_group": gsmall, "mid_group": gmid, "tuned": 1}
         # cached: a second call reuses it (and still matches)
         out2, sums2, _ = g.batch_run("bfs", src, tune=True)
         assert np.array_equal(sums, sums2)
@@ -157,3 +161,60 @@ def test_direct_launches_equal_graph_replays(T, O, g14w, monkeypatch):
                            for a in ("bfs", "sssp")]
     for a, b in zip(res["0"], res["1"]):
         assert np.array_equal(a, b)
+
+
+@pytest.fixture(scope="module")
+def skewed(O):
+    """Three degree populations: 40 hubs of out-degree 3000, 1,500 vertices
+    of out-degree 120, 18,460 of out-degree 3 (seeded uniform targets)."""
+    rng = np.random.default_rng(7)
+    nv = 20000
+    deg = np.full(nv, 3, np.int64)
+    perm = rng.permutation(nv)
+    deg[perm[:40]] = 3000
+    deg[perm[40:1540]] = 120
+    src = np.repeat(np.arange(nv), deg)
+    dst = rng.integers(0, nv, len(src))
+    g = O.from_edges(nv, src, dst)
+    return O.CSR(g.off, g.adj, O.weights(g))
+
+
+BUCKETS = [
+    dict(),                                                   # tuned / default
+    dict(small_degree=16, mid_degree=512, chunk_edges=256, small_group=32, mid_group=4),
+    dict(small_degree=16, mid_degree=512, chunk_edges=128, small_group=8, mid_group=1),
+    dict(small_degree=64, mid_degree=2048, chunk_edges=512, small_group=16, mid_group=2),
+    dict(small_degree=16, mid_degree=16, chunk_edges=128, small_group=1),  # two buckets
+]
+
+
+@pytest.mark.parametrize("algo", ["bfs", "sssp"])
+def test_degree_buckets_leave_results_unchanged(T, O, skewed, algo, tmp_path, monkeypatch):
+    monkeypatch.setenv("THV_TUNE_CACHE", str(tmp_path / "tune.txt"))
+    deg = np.diff(skewed.off.astype(np.int64))
+    # every bucket of the second configuration is populated
+    assert (deg < 16).sum() and ((deg >= 16) & (deg < 512)).sum() and (deg >= 512).sum()
+    src = sources(O, skewed, 64)
+    want = [O.bfs(skewed, int(s)) if algo == "bfs" else O.sssp(skewed, int(s)) for s in src]
+    edges = skewed.adj if algo == "bfs" else skewed.wcsr_edges()
+    with T.Graph.from_arrays(skewed.off, edges, "csr" if algo == "bfs" else "wcsr") as g:
+        g.plan(int(0.4 * g.ne * g.esz), block_bytes=BLOCK)
+        for cfg in BUCKETS:
+            out, sums, _ = g.batch_run(algo, src, timeout_ms=20000, **cfg)
+            for i, s in enumerate(src):
+                assert np.array_equal(out[i], want[i]), f"{cfg} source {s}"
+        # tuning times the buckets' settings and reports the one it keeps;
+        # the results stay those of the single-source runs
+        assert g.batch_tuned(algo)["tuned"] == 0
+        out, sums, _ = g.batch_run(algo, src, timeout_ms=20000, tune=True)
+        for i, s in enumerate(src):
+            assert np.array_equal(out[i], want[i]), f"tuned, source {s}"
+        c = g.batch_tuned(algo)
+        assert c["tuned"] == 1
+        assert 16 <= c["small_degree"] <= c["mid_degree"]
+        assert c["threads"] in (256, 512) and c["chunk_edges"] >= 128
+        # the buckets get different configurations: grouped vertices share a
+        # warp (small_group of them), chunked ones spread over several warps
+        assert c["small_group"] >= 1 and c["chunk_edges"] < 3000
+        if c["mid_degree"] > c["small_degree"]:
+            assert c["mid_group"] < c["small_group"]

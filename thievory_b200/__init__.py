@@ -95,7 +95,19 @@ class _BatchOpts(ctypes.Structure):
     _fields_ = [("group", ctypes.c_uint32), ("timeout_ms", ctypes.c_uint32),
                 ("stream", ctypes.c_void_p), ("small_degree", ctypes.c_uint32),
                 ("chunk_edges", ctypes.c_uint32), ("sssp_delta", ctypes.c_uint32),
-                ("tune", ctypes.c_uint32), ("sssp_growth", ctypes.c_uint32)]
+                ("tune", ctypes.c_uint32), ("sssp_growth", ctypes.c_uint32),
+                ("mid_degree", ctypes.c_uint32), ("small_group", ctypes.c_uint32),
+                ("mid_group", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+
+class _BatchConfig(ctypes.Structure):
+    _fields_ = [("small_degree", ctypes.c_uint32), ("mid_degree", ctypes.c_uint32),
+                ("chunk_edges", ctypes.c_uint32), ("threads", ctypes.c_uint32),
+                ("small_group", ctypes.c_uint32), ("mid_group", ctypes.c_uint32),
+                ("tuned", ctypes.c_uint32), ("pad", ctypes.c_uint32)]
+
+    def to_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "pad"}
 
 
 class _ServeOpts(ctypes.Structure):
@@ -121,7 +133,7 @@ class _QueryStats(ctypes.Structure):
 ABI_FUNCTIONS = [
     "thv_open", "thv_from_arrays", "thv_generate_rmat", "thv_save", "thv_close",
     "thv_info", "thv_set_edge_packing", "thv_set_symmetric", "thv_convert", "thv_host_arrays", "thv_plan", "thv_get_plan", "thv_get_blocks", "thv_get_block_access", "thv_save_plan", "thv_load_plan", "thv_run",
-    "thv_values", "thv_write_values", "thv_batch_run", "thv_serve_start",
+    "thv_values", "thv_write_values", "thv_batch_run", "thv_batch_tuned", "thv_serve_start",
     "thv_serve_submit", "thv_serve_poll", "thv_serve_wait", "thv_serve_stop",
     "thv_pick_sources", "thv_bfs_noalloc", "thv_link_bandwidth", "thv_last_error", "thv_status_str", "thv_abi_version",
     "thv_debug_fail_alloc_after", "thv_debug_wait_timeout",
@@ -167,6 +179,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "thv_write_values": ([ctypes.c_char_p, P, U64, U32], I32),
         "thv_batch_run": ([P, U32, P, U32, ctypes.POINTER(_BatchOpts), P, P,
                            ctypes.POINTER(_Stats)], I32),
+        "thv_batch_tuned": ([P, U32, ctypes.POINTER(_BatchConfig)], I32),
         "thv_serve_start": ([P, ctypes.POINTER(_ServeOpts), pp], I32),
         "thv_serve_submit": ([P, U32, U32, P, ctypes.POINTER(ctypes.c_uint64)], I32),
         "thv_serve_poll": ([P, U64, ctypes.POINTER(_QueryStats)], I32),
@@ -360,19 +373,33 @@ class Graph:
     def batch_run(self, algo: str, sources: Sequence[int], group: int = 64,
                   want_values: bool = True, stream: int = 0, small_degree: int = 0,
                   chunk_edges: int = 0, timeout_ms: int = 0, sssp_delta: int = 0,
-                  tune: bool = False, sssp_growth: int = 0):
-        """Batched BFS/SSSP; returns (values [n, nv] or None, checksums [n], stats)."""
+                  tune: bool = False, sssp_growth: int = 0, mid_degree: int = 0,
+                  small_group: int = 0, mid_group: int = 0):
+        """Batched BFS/SSSP; returns (values [n, nv] or None, checksums [n], stats).
+
+        small_degree / mid_degree / chunk_edges / small_group / mid_group set
+        the degree buckets of the expansion explicitly (thv_batch_opts); all
+        zero takes the tuned configuration (tune=True tunes it on the first
+        group when none is cached) or the default."""
         lib = load_library()
         src = np.ascontiguousarray(sources, dtype=np.uint32)
         out = np.empty((len(src), self.nv), dtype=np.uint32) if want_values else None
         sums = np.empty(len(src), dtype=np.uint64)
         o = _BatchOpts(group, timeout_ms, ctypes.c_void_p(stream) if stream else None,
-                       small_degree, chunk_edges, sssp_delta, 1 if tune else 0, sssp_growth)
+                       small_degree, chunk_edges, sssp_delta, 1 if tune else 0, sssp_growth,
+                       mid_degree, small_group, mid_group, 0)
         st = _Stats()
         _check(lib.thv_batch_run(self._h, ALGO[algo], _ptr(src), len(src), ctypes.byref(o),
                                  None if out is None else _ptr(out), _ptr(sums),
                                  ctypes.byref(st)), f"thv_batch_run({algo})")
         return out, sums, st.to_dict()
+
+    def batch_tuned(self, algo: str) -> dict:
+        """The batch kernel's configuration for this graph (thv_batch_tuned)."""
+        c = _BatchConfig()
+        _check(load_library().thv_batch_tuned(self._h, ALGO[algo], ctypes.byref(c)),
+               f"thv_batch_tuned({algo})")
+        return c.to_dict()
 
     def pick_sources(self, n: int, seed: int = 0x54484592) -> np.ndarray:
         """n seeded sources uniform over vertices with out-degree > 0."""

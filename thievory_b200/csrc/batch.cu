@@ -55,7 +55,7 @@ __host__ __device__ __forceinline__ uint32_t row_pos(uint32_t s) {
 struct MsCtrl {
   GridBar bar;
   unsigned err, iters;
-  unsigned long long cnt_small[3], cnt_big[3], remaining[3], wc[3];
+  unsigned long long cnt_small[3], cnt_big[3], remaining[3], wc[3], cnt_mid[3];
   unsigned minkept[3], pad;
   unsigned long long edges, hbm_bytes, link_bytes, pairs;
   // live groups: where a launch that yielded stopped (the next launch
@@ -77,14 +77,17 @@ struct MsArgs {
   uint32_t *dist;             // SSSP [nv][64]: distance + 1
   uint32_t *bm;
   uint32_t *wmin;             // SSSP: lower bound of pending distances per word
-  WorkItem *qs, *qb;
-  unsigned long long *qsm, *qbm;  // masks of the queued items
+  WorkItem *qs, *qb, *qm;
+  unsigned long long *qsm, *qbm, *qmm;  // masks of the queued items
   unsigned long long cap_s, cap_b;
   MsCtrl *ctrl;
   const uint32_t *sources;  // [k, source 0, ..., source k-1]
   unsigned long long timeout_ns;
   uint32_t nblk, nv, ngroups, max_iters;
+  // degree buckets: [1, small_deg) in groups of gsmall vertices per warp,
+  // [small_deg, mid_deg) in groups of gmid, the rest in chunk-edge items
   uint32_t small_deg, chunk, delta;
+  uint32_t mid_deg, gsmall, gmid;
   uint32_t wshift, wbase;  // packed weighted edges (see edge_dst / edge_wt)
   uint32_t growth;         // SSSP window width factor per advance
   // live groups: a launch returns at the top of iteration yield_at (0 =
@@ -101,8 +104,8 @@ struct BatchState {
   uint8_t *d_lvl = nullptr;
   uint32_t *d_dist = nullptr;
   uint32_t *d_bm = nullptr, *d_wmin = nullptr;
-  WorkItem *d_qs = nullptr, *d_qb = nullptr;
-  unsigned long long *d_qsm = nullptr, *d_qbm = nullptr;
+  WorkItem *d_qs = nullptr, *d_qb = nullptr, *d_qm = nullptr;
+  unsigned long long *d_qsm = nullptr, *d_qbm = nullptr, *d_qmm = nullptr;
   uint64_t cap_s = 0, cap_b = 0;
   MsCtrl *d_ctrl = nullptr, *h_ctrl = nullptr;
   uint32_t *d_sources = nullptr, *h_sources = nullptr;
@@ -360,16 +363,21 @@ __device__ __forceinline__ void ms_chunk(const MsArgs &a, uint32_t ring, const W
   }
 }
 
+// Up to gsize queued vertices per warp (q, qmask: the small or the medium
+// bucket's queue): lanes share their concatenated adjacency, so a vertex
+// gets about 32 / gsize lanes.
 template <int OP, int ESZ>
-__device__ __forceinline__ void ms_group(const MsArgs &a, uint32_t ring, unsigned long long first,
-                                         unsigned long long n_small, uint32_t lvl1) {
+__device__ __forceinline__ void ms_group(const MsArgs &a, uint32_t ring, const WorkItem *q,
+                                         const unsigned long long *qmask, unsigned long long first,
+                                         unsigned long long n_items, unsigned gsize,
+                                         uint32_t lvl1) {
   const unsigned lane = lane_id();
   const unsigned long long idx = first + lane;
   WorkItem it{0, 0, 0};
   unsigned long long f = 0;
-  if (idx < n_small) {
-    it = a.qs[idx];
-    f = a.qsm[idx];
+  if (lane < gsize && idx < n_items) {
+    it = q[idx];
+    f = qmask[idx];
   }
   if (OP == MS_SSSP) {
     // items with dense masks: one at a time, lanes = sources
@@ -483,6 +491,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
     if (leader) {
       c->cnt_small[nslot] = 0;
       c->cnt_big[nslot] = 0;
+      c->cnt_mid[nslot] = 0;
       c->remaining[nslot] = 0;
       c->wc[nslot] = 0;
       c->minkept[nslot] = 0xFFFFFFFFu;
@@ -564,7 +573,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
           else my_hbm += (unsigned long long)deg * ESZ;
         }
         const bool small = take && deg > 0 && deg < a.small_deg;
-        const bool big = take && deg >= a.small_deg;
+        const bool mid = take && deg >= a.small_deg && deg < a.mid_deg;
+        const bool big = take && deg >= max(a.small_deg, a.mid_deg);
         const unsigned sm = __ballot_sync(kFull, small);
         if (sm) {
           const int ldr = __ffs(sm) - 1;
@@ -577,6 +587,23 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
             if (pos < a.cap_s) {
               a.qs[pos] = WorkItem{eaddr, v, deg};
               a.qsm[pos] = take;
+            } else {
+              atomicCAS(&c->err, 0u, kDevErrQueue);
+            }
+          }
+        }
+        const unsigned mm = __ballot_sync(kFull, mid);
+        if (mm) {
+          const int ldr = __ffs(mm) - 1;
+          unsigned long long base = 0;
+          if (lane == (unsigned)ldr)
+            base = atomicAdd(&c->cnt_mid[slot], (unsigned long long)__popc(mm));
+          base = shfl64(base, ldr);
+          const unsigned long long pos = base + __popc(mm & lanemask_lt());
+          if (mid) {
+            if (pos < a.cap_s) {
+              a.qm[pos] = WorkItem{eaddr, v, deg};
+              a.qmm[pos] = take;
             } else {
               atomicCAS(&c->err, 0u, kDevErrQueue);
             }
@@ -625,7 +652,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
     const unsigned long long ns = ldcg(&c->cnt_small[slot]);
     const unsigned long long nb = ldcg(&c->cnt_big[slot]);
-    if (ns + nb == 0) {
+    const unsigned long long nm = ldcg(&c->cnt_mid[slot]);
+    if (ns + nb + nm == 0) {
       if (OP == MS_BFS) break;
       if (ldcg(&c->remaining[slot]) == 0) break;
       width = (uint32_t)min((unsigned long long)width * a.growth, 0xFFFFFFFFull);
@@ -634,10 +662,12 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
     }
     // ----------------------------------------------------------- expansion
     const uint32_t lvl1 = level + 1;
-    const unsigned long long ntask = nb + (ns + 31) / 32;
+    const unsigned long long nmt = (nm + a.gmid - 1) / a.gmid;
+    const unsigned long long ntask = nb + nmt + (ns + a.gsmall - 1) / a.gsmall;
     for (unsigned long long t = gwarp; t < ntask;) {
       if (t < nb) ms_chunk<OP, ESZ>(a, ring, a.qb[t], a.qbm[t], lvl1);
-      else ms_group<OP, ESZ>(a, ring, (t - nb) * 32ull, ns, lvl1);
+      else if (t < nb + nmt) ms_group<OP, ESZ>(a, ring, a.qm, a.qmm, (t - nb) * a.gmid, nm, a.gmid, lvl1);
+      else ms_group<OP, ESZ>(a, ring, a.qs, a.qsm, (t - nb - nmt) * a.gsmall, ns, a.gsmall, lvl1);
       unsigned long long nt = 0;
       if (lane == 0) nt = nwarps + atomicAdd(&c->wc[slot], 1ull);
       t = shfl64(nt, 0);
@@ -976,31 +1006,38 @@ __global__ void ms_live_column(MsArgs a, uint32_t s, uint32_t b, uint32_t *out) 
 // (below: 32 vertices per warp, one thread per vertex with warp-cooperative
 // load balancing; at or above: chunks of `chunk` edges per warp) and the
 // threads per CTA.
+// Launch configuration of the batch kernel, per degree bucket:
+//   [1, small)    groups of gsmall vertices per warp (about 32 / gsmall
+//                 lanes per vertex, load-balanced over their edges);
+//   [small, mid)  groups of gmid vertices per warp (empty when mid <= small);
+//   [mid, ...)    chunks of `chunk` edges, one warp each;
+// and the threads per CTA of the one persistent launch.
 struct MsConfig {
-  uint32_t small, chunk, threads;
+  uint32_t small, chunk, threads, mid, gsmall, gmid;
   bool operator<(const MsConfig &o) const {
-    return std::tie(small, chunk, threads) < std::tie(o.small, o.chunk, o.threads);
+    return std::tie(small, chunk, threads, mid, gsmall, gmid) <
+           std::tie(o.small, o.chunk, o.threads, o.mid, o.gsmall, o.gmid);
   }
 };
 
-constexpr MsConfig kMsDefault{64, 256, 512};
-// candidates the autotuner times (one real group each)
-const MsConfig kMsCandidates[] = {{16, 128, 512}, {64, 256, 512}, {256, 512, 512},
-                                  {64, 1024, 512}, {16, 128, 256}, {64, 256, 256},
-                                  {256, 512, 256}, {64, 1024, 256}};
+constexpr MsConfig kMsDefault{64, 256, 512, 64, 32, 4};
 constexpr uint32_t kMsMinSmall = 16, kMsMinChunk = 128;
+// Grouped buckets stop at 2^20 edges per vertex, so a warp's group (at most
+// 32 lists) counts its edges in 32 bits.
+constexpr uint32_t kMsMaxGroupedDeg = 1u << 20;
 
 // A captured launch sequence holds its kernel arguments by value, so the key
 // covers every argument that can differ between calls on one batch state.
 struct GraphKey {
   int op, esz, threads;
   bool out;
-  uint32_t small, chunk, delta, growth;
+  uint32_t small, chunk, delta, growth, mid, gsmall, gmid;
   unsigned long long timeout_ns;
   bool operator<(const GraphKey &o) const {
-    return std::tie(op, esz, threads, out, small, chunk, delta, growth, timeout_ns) <
-           std::tie(o.op, o.esz, o.threads, o.out, o.small, o.chunk, o.delta, o.growth,
-                    o.timeout_ns);
+    return std::tie(op, esz, threads, out, small, chunk, delta, growth, mid, gsmall, gmid,
+                    timeout_ns) <
+           std::tie(o.op, o.esz, o.threads, o.out, o.small, o.chunk, o.delta, o.growth, o.mid,
+                    o.gsmall, o.gmid, o.timeout_ns);
   }
 };
 
@@ -1038,6 +1075,8 @@ static void free_state(BatchState *&b) {
   dev_free(b->d_qb);
   dev_free(b->d_qsm);
   dev_free(b->d_qbm);
+  dev_free(b->d_qm);
+  dev_free(b->d_qmm);
   dev_free(b->d_ctrl);
   pinned_free(b->h_ctrl);
   dev_free(b->d_sources);
@@ -1096,6 +1135,8 @@ static thv_status fill_batch_state(thv_graph *g, BatchState *b, bool sssp, bool 
   THV_TRY(dev_alloc((void **)&b->d_wmin, nw_alloc * 4, "batch pending minima"));
   THV_TRY(dev_alloc((void **)&b->d_qs, b->cap_s * sizeof(WorkItem), "batch queue"));
   THV_TRY(dev_alloc((void **)&b->d_qsm, b->cap_s * 8, "batch queue masks"));
+  THV_TRY(dev_alloc((void **)&b->d_qm, b->cap_s * sizeof(WorkItem), "batch medium queue"));
+  THV_TRY(dev_alloc((void **)&b->d_qmm, b->cap_s * 8, "batch medium queue masks"));
   THV_TRY(dev_alloc((void **)&b->d_qb, b->cap_b * sizeof(WorkItem), "batch chunk queue"));
   THV_TRY(dev_alloc((void **)&b->d_qbm, b->cap_b * 8, "batch chunk masks"));
   THV_TRY(dev_alloc((void **)&b->d_ctrl, sizeof(MsCtrl), "batch control"));
@@ -1167,7 +1208,7 @@ static thv_status run_group(thv_graph *g, bool sssp, MsArgs &a, cudaStream_t st,
   BatchState *b = g->bs;
   BatchExtra &ex = g_extra[b];
   const GraphKey key{sssp ? 1 : 0, (int)g->esz, (int)cfg.threads, want_out, cfg.small, cfg.chunk,
-                     a.delta,     a.growth,    a.timeout_ns};
+                     a.delta,     a.growth,    a.mid_deg,      a.gsmall, a.gmid, a.timeout_ns};
   auto it = ex.graphs.find(key);
   if (it == ex.graphs.end() && ex.capture_ok) {
     cudaStream_t cs = nullptr;
@@ -1230,7 +1271,7 @@ static thv_status fallback_single(thv_graph *g, const uint32_t *src, uint32_t k,
 
 static std::string tune_key(const thv_graph *g, bool sssp) {
   char buf[160];
-  snprintf(buf, sizeof(buf), "%s nv=%llu ne=%llu esz=%u resident=%llu blocks=%zu sms=%d",
+  snprintf(buf, sizeof(buf), "%s3 nv=%llu ne=%llu esz=%u resident=%llu blocks=%zu sms=%d",
            sssp ? "sssp" : "bfs", (unsigned long long)g->nv, (unsigned long long)g->ne, g->esz,
            (unsigned long long)g->plan.resident_edge_bytes, g->plan.blocks.size(), g->num_sms);
   return buf;
@@ -1256,8 +1297,11 @@ static bool tune_lookup(const std::string &key, MsConfig *cfg) {
     if (!bar) continue;
     *bar = 0;
     MsConfig c{};
-    if (key == line && sscanf(bar + 1, "%u %u %u", &c.small, &c.chunk, &c.threads) == 3 &&
-        (c.threads == 256 || c.threads == 512) && c.small >= kMsMinSmall && c.chunk >= kMsMinChunk) {
+    if (key == line &&
+        sscanf(bar + 1, "%u %u %u %u %u %u", &c.small, &c.chunk, &c.threads, &c.mid, &c.gsmall,
+               &c.gmid) == 6 &&
+        (c.threads == 256 || c.threads == 512) && c.small >= kMsMinSmall && c.chunk >= kMsMinChunk &&
+        c.gsmall >= 1 && c.gsmall <= 32 && c.gmid >= 1 && c.gmid <= 32) {
       *cfg = c;
       found = true;
     }
@@ -1278,7 +1322,8 @@ static void tune_store(const std::string &key, const MsConfig &c) {
   }
   FILE *f = fopen(path.c_str(), "a");
   if (!f) return;
-  fprintf(f, "%s|%u %u %u\n", key.c_str(), c.small, c.chunk, c.threads);
+  fprintf(f, "%s|%u %u %u %u %u %u\n", key.c_str(), c.small, c.chunk, c.threads, c.mid, c.gsmall,
+          c.gmid);
   fclose(f);
 }
 
@@ -1304,6 +1349,8 @@ static MsArgs ms_args(thv_graph *g, BatchState *b, uint32_t timeout_ms) {
   a.qb = b->d_qb;
   a.qsm = b->d_qsm;
   a.qbm = b->d_qbm;
+  a.qm = b->d_qm;
+  a.qmm = b->d_qmm;
   a.cap_s = b->cap_s;
   a.cap_b = b->cap_b;
   a.ctrl = b->d_ctrl;
@@ -1314,6 +1361,31 @@ static MsArgs ms_args(thv_graph *g, BatchState *b, uint32_t timeout_ms) {
   a.ngroups = b->ngroups;
   a.max_iters = (uint32_t)std::min<uint64_t>(g->nv + 2, 0x7FFFFFF0ull) * 2 + 8;
   return a;
+}
+
+static void apply_config(MsArgs &a, const MsConfig &c) {
+  a.small_deg = std::min(std::max(c.small, kMsMinSmall), kMsMaxGroupedDeg);
+  a.chunk = std::max(c.chunk, kMsMinChunk);
+  a.mid_deg = std::min(std::max(c.mid, a.small_deg), kMsMaxGroupedDeg);
+  a.gsmall = std::min(std::max(c.gsmall, 1u), 32u);
+  a.gmid = std::min(std::max(c.gmid, 1u), 32u);
+}
+
+thv_status batch_config(thv_graph *g, thv_algo algo, thv_batch_config *out) {
+  if (algo != THV_ALGO_BFS && algo != THV_ALGO_SSSP)
+    return fail(THV_EINVAL, "batched runs support BFS and SSSP");
+  THV_TRY(ensure_plan(g));
+  MsConfig c = kMsDefault;
+  const bool tuned = tune_lookup(tune_key(g, algo == THV_ALGO_SSSP), &c);
+  out->small_degree = c.small;
+  out->mid_degree = std::max(c.mid, c.small);
+  out->chunk_edges = c.chunk;
+  out->threads = c.threads;
+  out->small_group = c.gsmall;
+  out->mid_group = c.gmid;
+  out->tuned = tuned ? 1u : 0u;
+  out->pad = 0;
+  return THV_OK;
 }
 
 thv_status run_batch(thv_graph *g, thv_algo algo, const uint32_t *sources,
@@ -1360,10 +1432,7 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
   thv_stats local{};
   uint32_t launches = 0;
   float dev_ms = 0.f;
-  auto set_cfg = [&](const MsConfig &c) {
-    a.small_deg = std::max(c.small, kMsMinSmall);
-    a.chunk = std::max(c.chunk, kMsMinChunk);
-  };
+  auto set_cfg = [&](const MsConfig &c) { apply_config(a, c); };
   auto one_group = [&](uint32_t first, uint32_t k, const MsConfig &cfg, float *ms_out,
                        bool *deep) -> thv_status {
     set_cfg(cfg);
@@ -1388,21 +1457,67 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
 
   // configuration: explicit, cached, autotuned on the first group, or default
   MsConfig cfg = kMsDefault;
-  if (o && (o->small_degree || o->chunk_edges)) {
+  if (o && (o->small_degree || o->chunk_edges || o->mid_degree || o->small_group || o->mid_group)) {
     cfg.small = o->small_degree ? o->small_degree : kMsDefault.small;
     cfg.chunk = o->chunk_edges ? std::max<uint32_t>(32, (o->chunk_edges + 31) / 32 * 32) : kMsDefault.chunk;
+    cfg.mid = o->mid_degree ? o->mid_degree : cfg.small;
+    cfg.gsmall = o->small_group ? std::min<uint32_t>(o->small_group, 32) : kMsDefault.gsmall;
+    cfg.gmid = o->mid_group ? std::min<uint32_t>(o->mid_group, 32) : kMsDefault.gmid;
   } else {
     const std::string key = tune_key(g, sssp);
     if (!tune_lookup(key, &cfg) && o && o->tune && n > 0) {
+      // Coordinate descent over the buckets, one real group timed per
+      // candidate: the chunk of the high-degree bucket, the small bucket's
+      // boundary, the medium bucket (its upper boundary and vertices per
+      // warp), the small bucket's vertices per warp, then threads per CTA.
       const uint32_t k = std::min(group, n);
       float best_ms = 1e30f;
-      for (const MsConfig &c : kMsCandidates) {
+      bool moot = false;
+      auto trial = [&](MsConfig c) -> thv_status {
+        if (moot) return THV_OK;
+        if (c.mid < c.small) c.mid = c.small;
         float ms_ = 0;
         bool deep = false;
         THV_TRY(one_group(0, k, c, &ms_, &deep));
-        if (deep) break;  // depth fallback: tuning this graph is moot
-        if (ms_ < best_ms) { best_ms = ms_; cfg = c; }
+        if (deep) moot = true;  // depth fallback: tuning this graph is moot
+        // a change has to win by 2%, above the run-to-run spread of a group
+        else if (ms_ < best_ms * (best_ms < 1e29f ? 0.98f : 1.f)) { best_ms = ms_; cfg = c; }
+        return THV_OK;
+      };
+      {
+        // warm-up: the first pass pays for cold caches and first launches
+        float ms_ = 0;
+        bool deep = false;
+        THV_TRY(one_group(0, k, kMsDefault, &ms_, &deep));
+        moot = deep;
       }
+      THV_TRY(trial(kMsDefault));
+      for (uint32_t ch : {512u, 1024u}) { MsConfig c = cfg; c.chunk = ch; THV_TRY(trial(c)); }
+      {
+        const MsConfig base = cfg;
+        for (uint32_t sm : {16u, 256u}) {
+          MsConfig c = base;
+          c.small = sm;
+          c.mid = base.mid == base.small ? sm : std::max(base.mid, sm);
+          THV_TRY(trial(c));
+        }
+      }
+      {
+        // a medium bucket above the small one, fewer vertices per warp
+        const MsConfig base = cfg;
+        for (uint32_t f : {4u, 16u}) {
+          MsConfig c = base;
+          c.mid = std::min(base.small * f, kMsMaxGroupedDeg);
+          c.gmid = 4;
+          if (c.mid > base.small) THV_TRY(trial(c));
+        }
+      }
+      if (cfg.mid > cfg.small) {
+        const MsConfig base = cfg;
+        for (uint32_t gm : {1u, 2u, 8u}) { MsConfig c = base; c.gmid = gm; THV_TRY(trial(c)); }
+      }
+      { MsConfig c = cfg; c.gsmall = 16; THV_TRY(trial(c)); }
+      { MsConfig c = cfg; c.threads = 256; THV_TRY(trial(c)); }
       tune_store(key, cfg);
     }
   }
@@ -1476,8 +1591,7 @@ static MsArgs live_args(thv_graph *g, const LiveGroup *lg, uint32_t timeout_ms) 
   MsArgs a = ms_args(g, g->bs, timeout_ms);
   a.delta = kMsDelta;
   a.growth = kMsGrowth;
-  a.small_deg = std::max(lg->small, kMsMinSmall);
-  a.chunk = std::max(lg->chunk, kMsMinChunk);
+  apply_config(a, MsConfig{lg->small, lg->chunk, lg->threads, lg->mid, lg->gsmall, lg->gmid});
   return a;
 }
 
@@ -1532,6 +1646,9 @@ thv_status live_add(thv_graph *g, LiveGroup *lg, uint32_t k, const uint32_t *sou
     lg->small = cfg.small;
     lg->chunk = cfg.chunk;
     lg->threads = cfg.threads;
+    lg->mid = cfg.mid;
+    lg->gsmall = cfg.gsmall;
+    lg->gmid = cfg.gmid;
     lg->iter = 0;
     lg->level = 1;
     lg->width = kMsDelta;

@@ -1091,6 +1091,14 @@ thv_status thv_batch_run(thv_graph *g, thv_algo algo, const uint32_t *sources,
   THV_GUARD_END
 }
 
+thv_status thv_batch_tuned(thv_graph *g, thv_algo algo, thv_batch_config *out) {
+  THV_GUARD_BEGIN
+  if (!g || !out) return fail(THV_EINVAL, "null argument");
+  THV_CUDA(cudaSetDevice(g->device));
+  return batch_config(g, algo, out);
+  THV_GUARD_END
+}
+
 static uint64_t mix64_host(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;

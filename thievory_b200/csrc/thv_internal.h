@@ -195,6 +195,7 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
                           uint32_t n, const thv_batch_opts *o, uint32_t *const *rows,
                           uint64_t *checksums, thv_stats *stats);
 void batch_free(thv_graph *g);
+thv_status batch_config(thv_graph *g, thv_algo algo, thv_batch_config *out);
 
 // Continuous batched group of the server (batch.cu): up to 64 sources of
 // one algorithm share a traversal that stays on the device; between
@@ -204,6 +205,7 @@ void batch_free(thv_graph *g);
 struct LiveGroup {
   bool sssp = false, running = false;
   uint32_t small = 64, chunk = 256, threads = 512;  // launch configuration
+  uint32_t mid = 64, gsmall = 32, gmid = 4;
   uint32_t iter = 0, level = 1, thr = 0, width = 0;  // where the next launch resumes
   unsigned long long active = 0;                     // mask bits in use
   uint32_t base[64] = {};  // per bit: BFS level byte / SSSP distance of its source vertex
