@@ -604,6 +604,7 @@ def run_c4(b, args, g_csr=None):
         ck = Clocks(b.dev).start()
         _, sums, bst = g.batch_run(algo, src, want_values=False, sssp_delta=dl, tune=True)
         clocks = ck.stop()
+        tuned = g.batch_tuned(algo)
         nplain = min(64, n)
         plain_ms, plain_bytes = [], []
         for i, s_ in enumerate(src[:nplain]):
@@ -618,7 +619,7 @@ def run_c4(b, args, g_csr=None):
             "sssp_delta": dl, "batched_ms_total": bst["device_ms"],
             "plain_ms_mean": statistics.mean(plain_ms), "queries": len(src),
             "groups": (len(src) + 63) // 64, "batched_iterations": bst["iterations"],
-            "batched_launches": bst["kernel_launches"],
+            "batched_launches": bst["kernel_launches"], "launch_config": tuned,
             "batched_link_bytes": bst["link_edge_bytes"],
             "batched_edge_bytes": bst["hbm_edge_bytes"] + bst["link_edge_bytes"],
             "plain_form_edge_bytes": statistics.mean(plain_bytes) * len(src),

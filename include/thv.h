@@ -236,6 +236,15 @@ typedef struct thv_run_opts {
  * neighbours of every vertex and the lists of vertices outside the largest
  * component only; this flag keeps min-label propagation.  Same labels. */
 #define THV_RUN_LABEL_PROPAGATION 16u
+/* PageRank with the reference engine's semantics instead of the
+ * fixed-iteration FP32 method: FP64 values, no dangling redistribution,
+ * rounds until no vertex changes by more than 1e-3.  Pull: r0 = 1/N,
+ * r = 0.15 + 0.85 * sum of r(u)/outdeg(u) over in-edges, recomputed only
+ * for vertices still active.  Push: residual form, r0 = 0.15.  Values agree
+ * with the reference's to its comparer's 1e-3 absolute tolerance (its FP64
+ * atomics make its own sums order-dependent).  pr_iters caps the rounds
+ * (0 = 100000; THV_ETIMEOUT when reached); stats->iterations = rounds. */
+#define THV_RUN_PR_REFERENCE 32u
 
 typedef struct thv_stats {
   double device_ms;         /* CUDA-event time of the traversal */

@@ -57,6 +57,8 @@ def lib() -> ctypes.CDLL:
             "thvo_sssp_par": ([U64, P, P, P, U32, U32, P], I),
             "thvo_pagerank": ([U64, P, P, U32, U32, D, P], I),
             "thvo_pagerank_csc": ([U64, P, P, P, U32, D, P], I),
+            "thvo_pagerank_ref_pull": ([U64, P, P, P, U32, P, P], I),
+            "thvo_pagerank_ref_push": ([U64, P, P, U32, U32, P, P], I),
             "thvo_reached_edges": ([U64, P, P], U64),
             "thvo_write_csr": ([ctypes.c_char_p, U64, U64, P, P, P], I),
             "thvo_write_csc": ([ctypes.c_char_p, U64, U64, P, P, P], I),
@@ -216,6 +218,31 @@ def pagerank_csc(in_off, in_adj, outdeg, iters: int = 20, damping: float = 0.85)
     if lib().thvo_pagerank_csc(nv, _p(in_off), _p(in_adj), _p(outdeg), iters, damping, _p(out)) != 0:
         raise MemoryError("pagerank_csc")
     return out
+
+
+def pagerank_ref_pull(in_off, in_adj, outdeg, max_rounds: int = 100000):
+    """The reference engine's pull PageRank (FP64, tolerance-driven) over a
+    CSC; returns (values, rounds)."""
+    nv = len(in_off) - 1
+    io, ia, od = _c(in_off, np.uint64), _c(in_adj, np.uint32), _c(outdeg, np.uint32)
+    out = np.empty(nv, np.float64)
+    rounds = np.zeros(1, np.uint32)
+    rc = lib().thvo_pagerank_ref_pull(nv, _p(io), _p(ia), _p(od), max_rounds, _p(out), _p(rounds))
+    if rc != 0:
+        raise RuntimeError(f"pagerank_ref_pull: {rc}")
+    return out, int(rounds[0])
+
+
+def pagerank_ref_push(g: CSR, max_rounds: int = 100000):
+    """The reference engine's push PageRank (FP64 residual form,
+    tolerance-driven) over the out-edges; returns (values, rounds)."""
+    out = np.empty(g.nv, np.float64)
+    rounds = np.zeros(1, np.uint32)
+    rc = lib().thvo_pagerank_ref_push(g.nv, _p(g.off), _p(g.adj), 1, max_rounds, _p(out),
+                                      _p(rounds))
+    if rc != 0:
+        raise RuntimeError(f"pagerank_ref_push: {rc}")
+    return out, int(rounds[0])
 
 
 def reached_edges(g: CSR, values: np.ndarray) -> int:

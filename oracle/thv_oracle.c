@@ -536,6 +536,107 @@ int thvo_pagerank(uint64_t nv, const uint64_t *off, const uint32_t *adj,
   return rc;
 }
 
+/* The reference's PageRank constants are floats (src/common.cuh:48-49,
+ * TOLERANCE 0.001f, ALPHA 0.85f); its expressions mix them with doubles, and
+ * the same C expressions below give the same promoted values. */
+static const float kRefAlpha = 0.85f, kRefTol = 0.001f;
+
+/* Pull: r0 = 1/N (src/graph.cuh:239-240); every round, each active vertex
+ * sums r(u)/outdeg(u) over its in-edges with the values of the previous
+ * round (the gather kernels, src/pr/pr_kernels.cu:23-55 and their demand /
+ * filter forms, all run before the update), then r = (1-a) + a*sum and the
+ * vertex stays active while |change| > tol (PR32_Update_Values,
+ * pr_kernels.cu:449-476); an inactive vertex never returns.  Rounds run while
+ * any vertex is active (src/pr/pr.cu:49-500). */
+int thvo_pagerank_ref_pull(uint64_t nv, const uint64_t *in_off,
+                           const uint32_t *in_adj, const uint32_t *outdeg,
+                           uint32_t max_rounds, double *rank, uint32_t *rounds) {
+  double *sum = (double *)malloc((nv + 1) * sizeof(double));
+  unsigned char *act = (unsigned char *)malloc(nv + 1);
+  if (!sum || !act) { free(sum); free(act); return -1; }
+  for (uint64_t v = 0; v < nv; v++) { rank[v] = 1.0 / (double)nv; act[v] = 1; }
+  uint64_t nact = nv;
+  uint32_t r = 0;
+  while (nact) {
+    if (r == max_rounds) { free(sum); free(act); *rounds = r; return -2; }
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t v = 0; v < (int64_t)nv; v++) {
+      if (!act[v]) continue;
+      double s = 0.0;
+      for (uint64_t i = in_off[v]; i < in_off[v + 1]; i++) {
+        const uint32_t u = in_adj[i];
+        if (outdeg[u]) s += rank[u] / (double)outdeg[u];
+      }
+      sum[v] = s;
+    }
+    nact = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nact)
+    for (int64_t v = 0; v < (int64_t)nv; v++) {
+      if (!act[v]) continue;
+      const double t = (1 - kRefAlpha) + kRefAlpha * sum[v];
+      const double diff = t > rank[v] ? t - rank[v] : rank[v] - t;
+      rank[v] = t;
+      act[v] = diff > kRefTol;
+      nact += act[v];
+    }
+    r++;
+  }
+  free(sum);
+  free(act);
+  *rounds = r;
+  return 0;
+}
+
+/* Push, residual form: r0 = 1-a, delta0 = (1-a)*a/outdeg computed in float,
+ * residual 0, every vertex active (src/graph.cuh:233-237).  Every round
+ * clears the frontier (src/pr/pr.cu:1067-1077), each active u adds delta(u)
+ * to residual(w) over its out-edges (PR32_Static_Kernel_PUSH and its demand /
+ * filter forms, pr_kernels.cu:504-681), then every vertex whose residual
+ * exceeds tol takes it: r += residual, delta = residual*a/outdeg,
+ * residual = 0, active (PR32_Update_Values_PUSH, pr_kernels.cu:846-860).
+ * Residuals at or under tol stay and keep accumulating. */
+int thvo_pagerank_ref_push(uint64_t nv, const uint64_t *off,
+                           const uint32_t *adj, uint32_t stride,
+                           uint32_t max_rounds, double *rank, uint32_t *rounds) {
+  double *delta = (double *)malloc((nv + 1) * sizeof(double));
+  double *res = (double *)malloc((nv + 1) * sizeof(double));
+  unsigned char *act = (unsigned char *)malloc(nv + 1);
+  if (!delta || !res || !act) { free(delta); free(res); free(act); return -1; }
+  for (uint64_t v = 0; v < nv; v++) {
+    rank[v] = (double)(1.0f - kRefAlpha);
+    delta[v] = (double)((1.0f - kRefAlpha) * kRefAlpha / (float)(off[v + 1] - off[v]));
+    res[v] = 0.0;
+    act[v] = 1;
+  }
+  uint64_t nact = nv;
+  uint32_t r = 0;
+  while (nact) {
+    if (r == max_rounds) { free(delta); free(res); free(act); *rounds = r; return -2; }
+    for (uint64_t u = 0; u < nv; u++) {
+      if (!act[u]) continue;
+      for (uint64_t i = off[u]; i < off[u + 1]; i++) res[adj[i * stride]] += delta[u];
+    }
+    nact = 0;
+    for (uint64_t v = 0; v < nv; v++) {
+      if (res[v] > kRefTol) {
+        rank[v] += res[v];
+        delta[v] = res[v] * kRefAlpha / (double)(off[v + 1] - off[v]);
+        res[v] = 0.0;
+        act[v] = 1;
+        nact++;
+      } else {
+        act[v] = 0;
+      }
+    }
+    r++;
+  }
+  free(delta);
+  free(res);
+  free(act);
+  *rounds = r;
+  return 0;
+}
+
 uint64_t thvo_reached_edges(uint64_t nv, const uint64_t *off,
                             const uint32_t *val) {
   uint64_t s = 0;

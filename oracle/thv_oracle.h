@@ -105,6 +105,18 @@ int thvo_pagerank_csc(uint64_t nv, const uint64_t *in_off,
                       const uint32_t *in_adj, const uint32_t *outdeg,
                       uint32_t iters, double damping, double *rank);
 
+/* PageRank with the reference engine's own semantics (FP64 values, rounds
+ * until no vertex changes by more than its tolerance, no dangling
+ * redistribution).  pull: in-edges (CSC) with explicit out-degrees;
+ * push: out-edges (CSR, residual form).  *rounds gets the number of rounds;
+ * returns -2 when max_rounds ran out. */
+int thvo_pagerank_ref_pull(uint64_t nv, const uint64_t *in_off,
+                           const uint32_t *in_adj, const uint32_t *outdeg,
+                           uint32_t max_rounds, double *rank, uint32_t *rounds);
+int thvo_pagerank_ref_push(uint64_t nv, const uint64_t *off,
+                           const uint32_t *adj, uint32_t adj_stride,
+                           uint32_t max_rounds, double *rank, uint32_t *rounds);
+
 /* Sum of out-degrees of vertices with value < nv+1 (edges a single-source
  * traversal must expand: the GTEPS numerator). */
 uint64_t thvo_reached_edges(uint64_t nv, const uint64_t *off,

@@ -346,15 +346,20 @@ class Graph:
             out: Optional[np.ndarray] = None, want_values: bool = True, stream: int = 0,
             sssp_delta: int = 0, timeout_ms: int = 0, small_degree: int = 0,
             chunk_edges: int = 0, checksum: bool = False, compaction: str = "",
-            sssp_growth: int = 0, top_down_only: bool = False, label_propagation: bool = False):
+            sssp_growth: int = 0, top_down_only: bool = False, label_propagation: bool = False,
+            pr_reference: bool = False, pr_max_rounds: int = 0):
         """Run algo; returns (values or None, stats dict).  compaction:
         "" (per-algorithm default), "scan" or "queue"; sssp_growth: SSSP
-        window growth per advance (0 = default 16, 1 = fixed windows)."""
+        window growth per advance (0 = default 16, 1 = fixed windows).
+        pr_reference: PageRank with the reference engine's semantics (FP64,
+        rounds until converged to 1e-3; THV_RUN_PR_REFERENCE), at most
+        pr_max_rounds rounds (0 = 100000)."""
         lib = load_library()
         flags = ((1 if checksum else 0) | (2 if compaction == "scan" else 0)
                  | (4 if compaction == "queue" else 0) | (8 if top_down_only else 0)
-                 | (16 if label_propagation else 0))
-        o = _RunOpts(source, pr_iters, pr_damping, sssp_delta, timeout_ms,
+                 | (16 if label_propagation else 0) | (32 if pr_reference else 0))
+        o = _RunOpts(source, pr_max_rounds if pr_reference else pr_iters, pr_damping, sssp_delta,
+                     timeout_ms,
                      ctypes.c_void_p(stream) if stream else None, small_degree, chunk_edges,
                      flags, sssp_growth)
         st = _Stats()

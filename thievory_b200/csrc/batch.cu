@@ -55,13 +55,14 @@ __host__ __device__ __forceinline__ uint32_t row_pos(uint32_t s) {
 struct MsCtrl {
   GridBar bar;
   unsigned err, iters;
-  unsigned long long cnt_small[3], cnt_big[3], remaining[3], wc[3], cnt_mid[3];
+  unsigned long long cnt_small[3], cnt_big[3], remaining[3], wc[3];
   unsigned minkept[3], pad;
   unsigned long long edges, hbm_bytes, link_bytes, pairs;
   // live groups: where a launch that yielded stopped (the next launch
   // resumes there), and the OR of the pending-source masks after it
   unsigned y_iter, y_level, y_thr, y_width, yielded, pad2;
   unsigned long long alive;
+  unsigned long long cnt_mid[3];  // kept off the line of the barrier and hot counters
 };
 
 struct MsArgs {
@@ -365,8 +366,9 @@ __device__ __forceinline__ void ms_chunk(const MsArgs &a, uint32_t ring, const W
 
 // Up to gsize queued vertices per warp (q, qmask: the small or the medium
 // bucket's queue): lanes share their concatenated adjacency, so a vertex
-// gets about 32 / gsize lanes.
-template <int OP, int ESZ>
+// gets about 32 / gsize lanes.  GS = 32 fixes gsize at compile time (the
+// two-bucket kernels); GS = 0 takes it from the argument.
+template <int OP, int ESZ, int GS>
 __device__ __forceinline__ void ms_group(const MsArgs &a, uint32_t ring, const WorkItem *q,
                                          const unsigned long long *qmask, unsigned long long first,
                                          unsigned long long n_items, unsigned gsize,
@@ -375,7 +377,7 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, uint32_t ring, const W
   const unsigned long long idx = first + lane;
   WorkItem it{0, 0, 0};
   unsigned long long f = 0;
-  if (lane < gsize && idx < n_items) {
+  if ((GS == 32 || lane < gsize) && idx < n_items) {
     it = q[idx];
     f = qmask[idx];
   }
@@ -440,7 +442,10 @@ __device__ __forceinline__ void ms_group(const MsArgs &a, uint32_t ring, const W
   }
 }
 
-template <int OP, int ESZ, int THREADS>
+// GS = 32: two degree buckets (small groups of 32 vertices per warp, chunks
+// above), the launch for the default and most tuned configurations; GS = 0:
+// three buckets with the groups' sizes from the arguments.
+template <int OP, int ESZ, int THREADS, int GS>
 __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
   // dynamic shared memory: SSSP's per-warp rings, then the block table
   extern __shared__ uint4 s_dyn[];
@@ -573,8 +578,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
           else my_hbm += (unsigned long long)deg * ESZ;
         }
         const bool small = take && deg > 0 && deg < a.small_deg;
-        const bool mid = take && deg >= a.small_deg && deg < a.mid_deg;
-        const bool big = take && deg >= max(a.small_deg, a.mid_deg);
+        const bool mid = GS == 0 && take && deg >= a.small_deg && deg < a.mid_deg;
+        const bool big = take && deg >= (GS == 0 ? max(a.small_deg, a.mid_deg) : a.small_deg);
         const unsigned sm = __ballot_sync(kFull, small);
         if (sm) {
           const int ldr = __ffs(sm) - 1;
@@ -592,7 +597,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
             }
           }
         }
-        const unsigned mm = __ballot_sync(kFull, mid);
+        const unsigned mm = GS == 0 && a.mid_deg > a.small_deg ? __ballot_sync(kFull, mid) : 0u;
         if (mm) {
           const int ldr = __ffs(mm) - 1;
           unsigned long long base = 0;
@@ -652,7 +657,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
     const unsigned long long ns = ldcg(&c->cnt_small[slot]);
     const unsigned long long nb = ldcg(&c->cnt_big[slot]);
-    const unsigned long long nm = ldcg(&c->cnt_mid[slot]);
+    const unsigned long long nm = GS == 0 ? ldcg(&c->cnt_mid[slot]) : 0ull;
     if (ns + nb + nm == 0) {
       if (OP == MS_BFS) break;
       if (ldcg(&c->remaining[slot]) == 0) break;
@@ -662,12 +667,19 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) ms_kernel(MsArgs a) {
     }
     // ----------------------------------------------------------- expansion
     const uint32_t lvl1 = level + 1;
-    const unsigned long long nmt = (nm + a.gmid - 1) / a.gmid;
-    const unsigned long long ntask = nb + nmt + (ns + a.gsmall - 1) / a.gsmall;
+    const unsigned gsmall = GS ? GS : a.gsmall;
+    const unsigned long long nmt = GS ? 0ull : (nm + a.gmid - 1) / a.gmid;
+    const unsigned long long ntask = nb + nmt + (ns + gsmall - 1) / gsmall;
     for (unsigned long long t = gwarp; t < ntask;) {
-      if (t < nb) ms_chunk<OP, ESZ>(a, ring, a.qb[t], a.qbm[t], lvl1);
-      else if (t < nb + nmt) ms_group<OP, ESZ>(a, ring, a.qm, a.qmm, (t - nb) * a.gmid, nm, a.gmid, lvl1);
-      else ms_group<OP, ESZ>(a, ring, a.qs, a.qsm, (t - nb - nmt) * a.gsmall, ns, a.gsmall, lvl1);
+      if (t < nb) {
+        ms_chunk<OP, ESZ>(a, ring, a.qb[t], a.qbm[t], lvl1);
+      } else {
+        // one inlined copy of the group code serves both grouped buckets
+        const bool md = GS == 0 && t < nb + nmt;
+        ms_group<OP, ESZ, GS>(a, ring, md ? a.qm : a.qs, md ? a.qmm : a.qsm,
+                              md ? (t - nb) * a.gmid : (t - nb - nmt) * gsmall, md ? nm : ns,
+                              md ? a.gmid : gsmall, lvl1);
+      }
       unsigned long long nt = 0;
       if (lane == 0) nt = nwarps + atomicAdd(&c->wc[slot], 1ull);
       t = shfl64(nt, 0);
@@ -1002,10 +1014,6 @@ __global__ void ms_live_column(MsArgs a, uint32_t s, uint32_t b, uint32_t *out) 
 
 // ------------------------------------------------------------------ host --
 
-// Launch configuration of the batch kernel: the degree-bucket boundary
-// (below: 32 vertices per warp, one thread per vertex with warp-cooperative
-// load balancing; at or above: chunks of `chunk` edges per warp) and the
-// threads per CTA.
 // Launch configuration of the batch kernel, per degree bucket:
 //   [1, small)    groups of gsmall vertices per warp (about 32 / gsmall
 //                 lanes per vertex, load-balanced over their edges);
@@ -1154,10 +1162,14 @@ static thv_status fill_batch_state(thv_graph *g, BatchState *b, bool sssp, bool 
 
 // The whole group -- sources up, reset, seed, persistent traversal,
 // extraction, status down -- enqueued on `st` (captured into a graph once).
+// The two-bucket kernel serves configurations without a medium bucket and
+// with 32 small vertices per warp.
+static bool two_buckets(const MsArgs &a) { return a.gsmall == 32 && a.mid_deg <= a.small_deg; }
+
 template <int OP, int ESZ, int THREADS>
 static thv_status enqueue_group(thv_graph *g, MsArgs &a, cudaStream_t st, bool want_out) {
   BatchState *b = g->bs;
-  auto kern = ms_kernel<OP, ESZ, THREADS>;
+  auto kern = two_buckets(a) ? ms_kernel<OP, ESZ, THREADS, 32> : ms_kernel<OP, ESZ, THREADS, 0>;
   const size_t ring = OP == MS_SSSP ? (size_t)THREADS / 32 * kMsRing * 512 : 0;
   const size_t smem = ring + (g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0);
   THV_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1480,8 +1492,9 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
         bool deep = false;
         THV_TRY(one_group(0, k, c, &ms_, &deep));
         if (deep) moot = true;  // depth fallback: tuning this graph is moot
-        // a change has to win by 2%, above the run-to-run spread of a group
-        else if (ms_ < best_ms * (best_ms < 1e29f ? 0.98f : 1.f)) { best_ms = ms_; cfg = c; }
+        // a change has to win by 0.5%, above the run-to-run spread of one
+        // group under one configuration (about 0.1%)
+        else if (ms_ < best_ms * (best_ms < 1e29f ? 0.995f : 1.f)) { best_ms = ms_; cfg = c; }
         return THV_OK;
       };
       {
@@ -1492,16 +1505,14 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
         moot = deep;
       }
       THV_TRY(trial(kMsDefault));
-      for (uint32_t ch : {512u, 1024u}) { MsConfig c = cfg; c.chunk = ch; THV_TRY(trial(c)); }
-      {
-        const MsConfig base = cfg;
-        for (uint32_t sm : {16u, 256u}) {
-          MsConfig c = base;
-          c.small = sm;
-          c.mid = base.mid == base.small ? sm : std::max(base.mid, sm);
-          THV_TRY(trial(c));
+      // the two-bucket grid: small-bucket boundary x chunk size
+      for (uint32_t sm : {16u, 64u, 256u})
+        for (uint32_t ch : {256u, 512u, 1024u}) {
+          MsConfig c = kMsDefault;
+          c.small = c.mid = sm;
+          c.chunk = ch;
+          if (sm != kMsDefault.small || ch != kMsDefault.chunk) THV_TRY(trial(c));
         }
-      }
       {
         // a medium bucket above the small one, fewer vertices per warp
         const MsConfig base = cfg;
@@ -1512,11 +1523,18 @@ thv_status run_batch_rows(thv_graph *g, thv_algo algo, const uint32_t *sources,
           if (c.mid > base.small) THV_TRY(trial(c));
         }
       }
+      // lanes per vertex: the medium bucket always gets more than the small
+      // one (fewer vertices per warp), 4 to 32
       if (cfg.mid > cfg.small) {
         const MsConfig base = cfg;
-        for (uint32_t gm : {1u, 2u, 8u}) { MsConfig c = base; c.gmid = gm; THV_TRY(trial(c)); }
+        for (uint32_t gm : {1u, 2u, 8u})
+          if (gm < base.gsmall) { MsConfig c = base; c.gmid = gm; THV_TRY(trial(c)); }
       }
-      { MsConfig c = cfg; c.gsmall = 16; THV_TRY(trial(c)); }
+      {
+        const MsConfig base = cfg;
+        for (uint32_t gs : {16u, 8u})
+          if (base.mid == base.small || gs > base.gmid) { MsConfig c = base; c.gsmall = gs; THV_TRY(trial(c)); }
+      }
       { MsConfig c = cfg; c.threads = 256; THV_TRY(trial(c)); }
       tune_store(key, cfg);
     }
@@ -1562,7 +1580,7 @@ constexpr uint64_t kLiveSsspRoom = 1ull << 24;
 template <int OP, int ESZ, int THREADS>
 static thv_status live_launch(thv_graph *g, MsArgs &a, cudaStream_t st) {
   BatchState *b = g->bs;
-  auto kern = ms_kernel<OP, ESZ, THREADS>;
+  auto kern = two_buckets(a) ? ms_kernel<OP, ESZ, THREADS, 32> : ms_kernel<OP, ESZ, THREADS, 0>;
   const size_t ring = OP == MS_SSSP ? (size_t)THREADS / 32 * kMsRing * 512 : 0;
   const size_t smem = ring + (g->plan.vbegin.size() <= kSmemBlocks + 1 ? g->plan.vbegin.size() * 4 : 0);
   THV_CUDA(cudaFuncSetAttribute((const void *)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

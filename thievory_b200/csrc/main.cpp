@@ -13,7 +13,9 @@
 //   dangling mass redistributed);
 //   no nvidia-smi / NUMA probing; errors are reported, with exit code 1.
 // Extra flags: --hbm-budget <bytes|N%|NK|NM|NG>, --block-bytes <bytes|NM>,
-//   --placement densest|prefix, --pr-iters N, --values <path>.
+//   --placement densest|prefix, --pr-iters N, --values <path>,
+//   --pr-semantics fixed|reference (fixed: FP32, --pr-iters iterations;
+//   reference: the reference engine's FP64 rounds to a 1e-3 tolerance).
 #include <sys/stat.h>
 
 #include <cstdio>
@@ -40,6 +42,7 @@ static void usage(const char *prog) {
   printf("  --placement : densest|prefix (default densest)\n");
   printf("  --symmetric : 1 = the graph has every reverse edge (CC by union-find)\n");
   printf("  --pr-iters : PageRank iterations (default 20)\n");
+  printf("  --pr-semantics : fixed|reference (default fixed; reference = FP64 to 1e-3)\n");
   printf("  --values : output path (default results/values.bin)\n");
 }
 
@@ -64,6 +67,7 @@ static int die(const char *what, thv_status s) {
 
 int main(int argc, char **argv) {
   std::string input, algo = "bfs", type = "push", budget, block, placement = "densest";
+  std::string pr_semantics = "fixed";
   std::string values_path = "results/values.bin";
   unsigned edge_size = 4, source = 1, runs = 1, gpus = 0, pr_iters = 20;
   int device = 0;
@@ -82,6 +86,7 @@ int main(int argc, char **argv) {
     else if (!strcmp(k, "--block-bytes")) block = v;
     else if (!strcmp(k, "--placement")) placement = v;
     else if (!strcmp(k, "--pr-iters")) pr_iters = (unsigned)atoi(v);
+    else if (!strcmp(k, "--pr-semantics")) pr_semantics = v;
     else if (!strcmp(k, "--values")) values_path = v;
     else if (!strcmp(k, "--symmetric")) symmetric = atoi(v) != 0;
     else { fprintf(stderr, "Error: unknown flag %s\n", k); usage(argv[0]); return 1; }
@@ -159,6 +164,14 @@ int main(int argc, char **argv) {
   thv_run_opts ro{};
   ro.source = source;
   ro.pr_iters = pr_iters;
+  if (pr_semantics == "reference") {
+    ro.flags |= THV_RUN_PR_REFERENCE;
+    ro.pr_iters = 0;
+  } else if (pr_semantics != "fixed") {
+    fprintf(stderr, "Error: wrong --pr-semantics\n");
+    thv_close(g);
+    return 1;
+  }
   double total_ms = 0;
   thv_stats st{};
   for (unsigned r = 0; r < runs; r++) {

@@ -949,18 +949,44 @@ constexpr int kScanPer = 4;
 // measured slower at RMAT-24).
 constexpr int kGroupPer = 8;
 
+// Appends the warp's staged vertices in batches of 32 lanes.  Unless all is
+// set, only whole batches go and the rest (fewer than 32) moves to the front
+// of the list, so a warp appends once per 32 queued vertices, however few
+// each relaxation step queues.  A vertex's queued bit is set when it is
+// staged; every staged vertex is appended before the phase's closing
+// barrier (the final call with all = true), so the bit still implies an
+// entry in this phase's queue.
+template <int ESZ>
+__device__ __forceinline__ void q_flush(const MinArgs &a, const QEnv &e, unsigned &nst, bool all,
+                                        QStats &qst) {
+  const unsigned lane = lane_id();
+  const unsigned take = all ? nst : (nst & ~31u);
+  if (!take) return;
+  __syncwarp();
+  for (unsigned k = 0; k < take; k += 32) {
+    const bool f = k + lane < take;
+    const uint2 x = f ? e.stage[k + lane] : make_uint2(0, 0);
+    q_append<ESZ>(a, e.vb, e.bbase, e.qs_next, e.qb_next, e.cs_next, f, x.x, x.y, qst);
+  }
+  const unsigned rest = nst - take;
+  const uint2 x = lane < rest ? e.stage[take + lane] : make_uint2(0, 0);
+  __syncwarp();
+  if (lane < rest) e.stage[lane] = x;
+  __syncwarp();
+  nst = rest;
+}
+
 // Relax N edges per lane; near improvements are queued, far ones parked.
-// Each dependent step (value probe, atomicMin, tag probe, tag atomicMax) is
-// issued for all N edges before any result is used, so a lane has N
-// requests in flight per step instead of one.  The vertices to queue are
-// staged in the warp's shared list and appended 32 at a time: one
-// warp-aggregated reservation per 32 queued vertices instead of one per
-// edge slot.  cand is the saturated u32 candidate (0xFFFFFFFF never wins).
+// Each dependent step (value probe, atomicMin, queued-bit claim) is issued
+// for all N edges before any result is used, so a lane has N requests in
+// flight per step instead of one.  The vertices to queue are staged in the
+// warp's shared list (nst entries, warp-uniform) and appended 32 at a time
+// by q_flush.  cand is the saturated u32 candidate (0xFFFFFFFF never wins).
 template <int OP, int ESZ, int N>
 __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const uint32_t (&w)[N],
                                           const uint32_t (&cand)[N], const bool (&ok)[N],
-                                          QStats &qst) {
-  static_assert(N <= kQRelaxMax, "staging list holds kQRelaxMax entries per lane");
+                                          unsigned &nst, QStats &qst) {
+  static_assert(N <= kQRelaxMax, "one step stages at most kQRelaxMax entries per lane");
   // values stay in L2 (evict-last) while edges and items stream through
   const unsigned long long keep = l2_evict_last();
   uint32_t r[N];
@@ -988,22 +1014,13 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
 #pragma unroll
     for (int j = 0; j < N; j++) push[j] = push[j] && !((r[j] >> (w[j] & 31u)) & 1u);
   }
-  const unsigned lane = lane_id();
-  unsigned n = 0;
 #pragma unroll
   for (int j = 0; j < N; j++) {
     const unsigned b = __ballot_sync(kFull, push[j]);
-    if (push[j]) e.stage[n + __popc(b & lanemask_lt())] = make_uint2(w[j], cand[j]);
-    n += __popc(b);
+    if (push[j]) e.stage[nst + __popc(b & lanemask_lt())] = make_uint2(w[j], cand[j]);
+    nst += __popc(b);
   }
-  if (!n) return;
-  __syncwarp();
-  for (unsigned k = 0; k < n; k += 32) {
-    const bool f = k + lane < n;
-    const uint2 x = f ? e.stage[k + lane] : make_uint2(0, 0);
-    q_append<ESZ>(a, e.vb, e.bbase, e.qs_next, e.qb_next, e.cs_next, f, x.x, x.y, qst);
-  }
-  __syncwarp();
+  if (nst >= 32) q_flush<ESZ>(a, e, nst, false, qst);
 }
 
 // Dequeue: BFS values are final when queued.  SSSP/CC clear the vertex's
@@ -1025,7 +1042,7 @@ __device__ __forceinline__ uint32_t q_dequeue(const MinArgs &a, const QEnv &e, u
 
 template <int OP, int ESZ>
 __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const MinItem &it,
-                                        QStats &qst) {
+                                        unsigned &nst, QStats &qst) {
   constexpr int PER = 16 / ESZ;
   const unsigned lane = lane_id();
   uint32_t vval = it.val;
@@ -1069,14 +1086,14 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
         cand[k] = sat32(candidate<OP>(vval, ESZ == 4 ? edge_wt(f[j], a.wshift, a.wbase) : f[2 * j + 1]));
       }
     }
-    q_relax_n<OP, ESZ, 2 * PER>(a, e, w, cand, ok, qst);
+    q_relax_n<OP, ESZ, 2 * PER>(a, e, w, cand, ok, nst, qst);
   }
 }
 
 template <int OP, int ESZ>
 __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const MinItem *qs,
                                         unsigned long long first, unsigned long long n_small,
-                                        QStats &qst) {
+                                        unsigned &nst, QStats &qst) {
   const unsigned lane = lane_id();
   const unsigned long long idx = first + lane;
   MinItem it{0, 0, 0};
@@ -1119,7 +1136,7 @@ __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const M
       }
       cand[h] = sat32(candidate<OP>(ov, wt));
     }
-    q_relax_n<OP, ESZ, kGroupPer>(a, e, w, cand, ok, qst);
+    q_relax_n<OP, ESZ, kGroupPer>(a, e, w, cand, ok, nst, qst);
   }
 }
 
@@ -1127,7 +1144,8 @@ template <int OP, int ESZ>
 // Two blocks per SM: 64 registers, no spills (3 blocks spill and measured slower).
 __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
   extern __shared__ unsigned long long s_tab[];
-  __shared__ uint2 s_stage[kMinThreads / 32][32 * kQRelaxMax];
+  // staging list: fewer than 32 carried entries plus one relaxation step's
+  __shared__ uint2 s_stage[kMinThreads / 32][32 * (kQRelaxMax + 1)];
   __shared__ uint32_t s_word[kMinThreads / 32][64];  // scan: taken bits, least kept value per word
   const bool smem_tab = a.nblk <= kSmemBlocks;
   unsigned long long *s_base = s_tab;
@@ -1266,17 +1284,19 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
       const unsigned long long ns = ldcg(&c->cnt_small[prev]);
       const unsigned long long nb = ldcg(&c->cnt_big[prev]);
       const unsigned long long ntask = nb + (ns + 31) / 32;
+      unsigned nst = 0;  // vertices staged in this warp's list, not yet appended
       for (unsigned long long t = gwarp; t < ntask;) {
         unsigned long long nt = 0;
         if (lane == 0) nt = atomicAdd(&c->wc[prev], 1ull);
         if (t < nb) {
           const MinItem it = qb_in[t];
-          q_chunk<OP, ESZ>(a, env, it, qst);
+          q_chunk<OP, ESZ>(a, env, it, nst, qst);
         } else {
-          q_group<OP, ESZ>(a, env, qs_in, (t - nb) * 32ull, ns, qst);
+          q_group<OP, ESZ>(a, env, qs_in, (t - nb) * 32ull, ns, nst, qst);
         }
         t = nwarps + shfl64(nt, 0);
       }
+      q_flush<ESZ>(a, env, nst, true, qst);
     }
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
     const unsigned long long produced = ldcg(&c->cnt_small[cur]) + ldcg(&c->cnt_big[cur]);
