@@ -1208,6 +1208,7 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
       unsigned long long my_keep = 0;
       uint32_t my_min = 0xFFFFFFFFu;
       uint32_t *s_tk = s_word[threadIdx.x >> 5], *s_km = s_tk + 32;
+      unsigned nst = 0;  // vertices staged in this warp's list, not yet appended
       for (unsigned g = gwarp; g < a.ngroups; g += nwarps) {
         const unsigned wbase = g * 32u;
         const uint32_t word = ldcg(a.bm + wbase + lane);
@@ -1240,7 +1241,6 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
           }
 #pragma unroll
           for (int i = 0; i < kScanPer; i++) vv[i] = v[i] != 0xFFFFFFFFu ? ldcg(a.val + v[i]) : 0u;
-          unsigned n = 0;
 #pragma unroll
           for (int i = 0; i < kScanPer; i++) {
             const bool in = v[i] != 0xFFFFFFFFu;
@@ -1248,15 +1248,10 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
             if (take) atomicOr(&s_tk[own[i]], 1u << (v[i] & 31u));
             else if (OP != OP_BFS && in) atomicMin(&s_km[own[i]], vv[i]);
             const unsigned b = __ballot_sync(kFull, take);
-            if (take) env.stage[n + __popc(b & lanemask_lt())] = make_uint2(v[i], vv[i]);
-            n += __popc(b);
+            if (take) env.stage[nst + __popc(b & lanemask_lt())] = make_uint2(v[i], vv[i]);
+            nst += __popc(b);
           }
-          __syncwarp();
-          for (unsigned kk = 0; kk < n; kk += 32) {
-            const bool f = kk + lane < n;
-            const uint2 x = f ? env.stage[kk + lane] : make_uint2(0, 0);
-            q_append<ESZ>(a, env.vb, env.bbase, qs_out, qb_out, cur, f, x.x, x.y, qst);
-          }
+          if (nst >= 32) q_flush<ESZ>(a, env, nst, false, qst);
           __syncwarp();
         }
         if (act_word) {
@@ -1271,6 +1266,7 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
         }
         __syncwarp();
       }
+      q_flush<ESZ>(a, env, nst, true, qst);
       if (OP != OP_BFS) {
         my_keep = warp_sum(my_keep);
         my_min = warp_min(my_min);
