@@ -47,6 +47,14 @@ enum { OP_BFS = 0, OP_CC = 1, OP_SSSP = 2 };
 constexpr int kMinThreads = 512;
 constexpr uint32_t kDefaultSmall = 64;  // degree < this: warp-cooperative
 constexpr uint32_t kDefaultChunk = 256; // edges per high-degree work item
+// Queue mode: one warp in this many (the link warps) drains the host-list
+// chunks of a phase first.  RMAT-24 SSSP, 40% HBM, mean over sources 1, 2,
+// 7 and 1000: every 3rd warp 7.41 ms, 4th 6.75, 5th 6.60, 6th 6.61, 8th
+// 6.90 (source 1: 6.23, 5.78, 5.68, 5.60, 5.56; every 16th: 6.24).  All
+// chunks in queue order took 5.96 / 7.73 / 8.18 ms at sources 1 / 7 / 1000
+// (every 6th: 5.60 / 6.95 / 7.43); no link warps (host chunks last) 7.27
+// ms at source 1.
+constexpr uint32_t kLinkEvery = 6;
 constexpr uint32_t kQueueChunkBytes = 4096;  // queue mode: bytes of edges per item (4 steps of 8 edges per lane when packed)
 // scan mode (BFS, CC): RMAT-20 BFS 0.408 -> 0.40 ms and RMAT-24 label
 // propagation 31.2 -> 30.1 ms with 1024 4-byte edges per item instead of 256
@@ -94,6 +102,9 @@ struct MinCtrl {
   // BFS: out-edges and size of each level's frontier; bottom-up levels run
   unsigned long long mf[3], nf[3], bu_scan[3];
   unsigned bu_levels, pad2;
+  // queue mode: chunk items of host-resident lists (counted apart, stored
+  // from the top of the chunk queue down) and their work counters
+  unsigned long long cnt_host[3], wc_host[3];
 };
 
 struct MinArgs {
@@ -127,6 +138,8 @@ struct MinArgs {
   uint32_t *bm2;
   unsigned long long ne;
   uint32_t do_alpha, do_beta;
+  // queue mode: one warp in link_every draws host-list chunks first (0: none)
+  uint32_t link_every, pad3;
 };
 
 struct MinState {
@@ -888,10 +901,10 @@ __device__ __forceinline__ void q_append(const MinArgs &a, const uint32_t *vb,
   const unsigned lane = lane_id();
   uint32_t deg = 0;
   unsigned long long eaddr = 0;
+  bool host = false;
   if (flag) {
     const uint64_t s0 = __ldg(a.off + w), e0 = __ldg(a.off + w + 1);
     deg = (uint32_t)(e0 - s0);
-    bool host;
     const uint32_t bi = find_block(vb, a.nblk, w);
     eaddr = list_addr(a.lc, bbase[bi], a.host_base, w, s0, deg, ESZ, &host);
     if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
@@ -910,19 +923,28 @@ __device__ __forceinline__ void q_append(const MinArgs &a, const uint32_t *vb,
       else atomicCAS(&c->err, 0u, kDevErrQueue);
     }
   }
-  if (__any_sync(kFull, big)) {
-    const unsigned nch = big ? (deg + a.chunk - 1) / a.chunk : 0u;
+  // chunks of HBM lists fill the chunk queue from the bottom, chunks of
+  // host-resident lists from the top (the expansion hands them to the
+  // link warps first); the two counts together stay within cap_b, which
+  // every block checks after the phase's barrier, before any item is read
+#pragma unroll
+  for (int on_host = 0; on_host < 2; on_host++) {
+    const bool mine = big && host == (on_host != 0);
+    if (!__any_sync(kFull, mine)) continue;
+    const unsigned nch = mine ? (deg + a.chunk - 1) / a.chunk : 0u;
     const unsigned inc = warp_incl_scan<unsigned>(nch);
     const unsigned tot = __shfl_sync(kFull, inc, 31);
     unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(&c->cnt_big[cs], (unsigned long long)tot);
+    if (lane == 0)
+      base = atomicAdd(on_host ? &c->cnt_host[cs] : &c->cnt_big[cs], (unsigned long long)tot);
     base = shfl64(base, 0);
-    if (big) {
+    if (mine) {
       unsigned long long pos = base + inc - nch;
       for (unsigned k = 0; k < nch; k++, pos++) {
         const uint32_t lo = k * a.chunk;
         if (pos < a.cap_b)
-          qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, min(a.chunk, deg - lo), w, wval);
+          qb[on_host ? a.cap_b - 1 - pos : pos] =
+              make_item(eaddr + (unsigned long long)lo * ESZ, min(a.chunk, deg - lo), w, wval);
         else
           atomicCAS(&c->err, 0u, kDevErrQueue);
       }
@@ -1045,6 +1067,25 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
                                         unsigned &nst, QStats &qst) {
   constexpr int PER = 16 / ESZ;
   const unsigned lane = lane_id();
+  const uintptr_t start = it.ea_cnt & kAddrMask;
+  const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
+  // two 16-byte loads per lane in flight (1 KiB per warp step): host-link
+  // reads are latency-bound per warp.  The next step's loads are issued
+  // before this step's relaxation, so they travel while its probes and
+  // atomics do.  An HBM chunk's first loads also go out before the
+  // dequeue's, which they do not depend on (a skipped item wastes 1 KiB of
+  // HBM reads); a host chunk's wait for the dequeue, so that skipped items
+  // cost no link bytes.
+  // edges are read once: evict-first
+  const unsigned long long stream = l2_evict_first();
+  const bool on_link = start >= a.host_base && start < a.host_end;
+  uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane;
+  uint4 qn[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+  if (!on_link) {
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+      if (p + 512u * h < end) qn[h] = ld_stream_v4(p + 512u * h, stream);
+  }
   uint32_t vval = it.val;
   if (OP != OP_BFS) {
     bool skip = false;
@@ -1052,20 +1093,12 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
     vval = __shfl_sync(kFull, vval, 0);
     if (__shfl_sync(kFull, skip, 0)) return;
   }
-  const uintptr_t start = it.ea_cnt & kAddrMask;
-  const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
   if (lane == 0) q_count(a, qst, start, (unsigned)(it.ea_cnt >> 48), ESZ);
-  // two 16-byte loads per lane in flight (1 KiB per warp step): host-link
-  // reads are latency-bound per warp.  The next step's loads are issued
-  // before this step's relaxation, so they travel while its probes and
-  // atomics do.
-  // edges are read once: evict-first
-  const unsigned long long stream = l2_evict_first();
-  uintptr_t p = (start & ~(uintptr_t)127) + 16u * lane;
-  uint4 qn[2];
+  if (on_link) {
 #pragma unroll
-  for (int h = 0; h < 2; h++)
-    qn[h] = p + 512u * h < end ? ld_stream_v4(p + 512u * h, stream) : make_uint4(0, 0, 0, 0);
+    for (int h = 0; h < 2; h++)
+      if (p + 512u * h < end) qn[h] = ld_stream_v4(p + 512u * h, stream);
+  }
   for (; __any_sync(kFull, p < end); p += 1024u) {
     uint4 q[2] = {qn[0], qn[1]};
 #pragma unroll
@@ -1186,7 +1219,9 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
       const unsigned r = (ph + 1) % 3;
       c->cnt_small[r] = 0;
       c->cnt_big[r] = 0;
+      c->cnt_host[r] = 0;
       c->wc[r] = 0;
+      c->wc_host[r] = 0;
       c->remaining[r] = 0;
       c->minkept[r] = 0xFFFFFFFFu;
     }
@@ -1277,25 +1312,60 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
       }
     } else {
       // --------------------------------------------------------- expansion
+      // Two task pools: chunks of host-resident lists (read over the
+      // link), and the rest (HBM chunks, then groups of small vertices).
+      // One warp in link_every (the link warps) drains the host pool
+      // first, so the link is busy from the phase's start while the other
+      // warps work through HBM-resident lists; each warp then helps with
+      // the other pool.  The first task of a warp's first pool is static
+      // (its index among that pool's warps), the rest come from the pool's
+      // counter.
       const unsigned long long ns = ldcg(&c->cnt_small[prev]);
       const unsigned long long nb = ldcg(&c->cnt_big[prev]);
+      const unsigned long long nh = ldcg(&c->cnt_host[prev]);
       const unsigned long long ntask = nb + (ns + 31) / 32;
+      const unsigned le = a.link_every;
+      const unsigned nlink = le ? (nwarps + le - 1) / le : 0u;
+      const bool link_warp = le && gwarp % le == 0;
       unsigned nst = 0;  // vertices staged in this warp's list, not yet appended
-      for (unsigned long long t = gwarp; t < ntask;) {
-        unsigned long long nt = 0;
-        if (lane == 0) nt = atomicAdd(&c->wc[prev], 1ull);
-        if (t < nb) {
-          const MinItem it = qb_in[t];
-          q_chunk<OP, ESZ>(a, env, it, nst, qst);
+#pragma unroll 1
+      for (int pass = 0; pass < 2; pass++) {
+        const bool hpool = link_warp == (pass == 0);
+        unsigned long long *ctr = hpool ? &c->wc_host[prev] : &c->wc[prev];
+        const unsigned long long n = hpool ? nh : ntask;
+        const unsigned long long first = hpool ? nlink : nwarps - nlink;
+        unsigned long long t;
+        if (pass == 0) {
+          t = link_warp ? gwarp / le : gwarp - (le ? gwarp / le + 1 : 0u);
         } else {
-          q_group<OP, ESZ>(a, env, qs_in, (t - nb) * 32ull, ns, nst, qst);
+          unsigned long long f = 0;
+          if (lane == 0 && first < n) f = atomicAdd(ctr, 1ull);
+          t = first + shfl64(f, 0);
         }
-        t = nwarps + shfl64(nt, 0);
+        while (t < n) {
+          unsigned long long nt = 0;
+          if (lane == 0) nt = atomicAdd(ctr, 1ull);
+          if (hpool) {
+            const MinItem it = qb_in[a.cap_b - 1 - t];
+            q_chunk<OP, ESZ>(a, env, it, nst, qst);
+          } else if (t < nb) {
+            const MinItem it = qb_in[t];
+            q_chunk<OP, ESZ>(a, env, it, nst, qst);
+          } else {
+            q_group<OP, ESZ>(a, env, qs_in, (t - nb) * 32ull, ns, nst, qst);
+          }
+          t = first + shfl64(nt, 0);
+        }
       }
       q_flush<ESZ>(a, env, nst, true, qst);
     }
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
-    const unsigned long long produced = ldcg(&c->cnt_small[cur]) + ldcg(&c->cnt_big[cur]);
+    const unsigned long long nbig = ldcg(&c->cnt_big[cur]), nhost = ldcg(&c->cnt_host[cur]);
+    if (nbig + nhost > a.cap_b) {  // the two ends of the chunk queue met
+      if (leader) atomicCAS(&c->err, 0u, kDevErrQueue);
+      break;
+    }
+    const unsigned long long produced = ldcg(&c->cnt_small[cur]) + nbig + nhost;
     if (produced) {
       scan = false;  // expand what this phase queued
     } else if (!scan) {
@@ -1744,6 +1814,7 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
   a.chunk = chunk;
   a.src = src;
   a.ne = g->ne;
+  a.link_every = kLinkEvery;
 
   // scan-built queues keep vertex order (coalesced offset reads) and no
   // fences: better for BFS and CC; SSSP gains from fewer barriers
