@@ -213,7 +213,7 @@ typedef struct thv_run_opts {
   uint32_t small_degree; /* expansion tuning; 0 = default */
   uint32_t chunk_edges;  /* expansion tuning; 0 = default */
   uint32_t flags;        /* THV_RUN_* */
-  uint32_t sssp_growth;  /* SSSP window width factor per advance: 0 = 16,
+  uint32_t sssp_growth;  /* SSSP window width factor per advance: 0 = 32,
                             1 = fixed windows (plain near/far) */
 } thv_run_opts;
 

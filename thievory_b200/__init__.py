@@ -350,7 +350,7 @@ class Graph:
             pr_reference: bool = False, pr_max_rounds: int = 0):
         """Run algo; returns (values or None, stats dict).  compaction:
         "" (per-algorithm default), "scan" or "queue"; sssp_growth: SSSP
-        window growth per advance (0 = default 16, 1 = fixed windows).
+        window growth per advance (0 = default 32, 1 = fixed windows).
         pr_reference: PageRank with the reference engine's semantics (FP64,
         rounds until converged to 1e-3; THV_RUN_PR_REFERENCE), at most
         pr_max_rounds rounds (0 = 100000)."""

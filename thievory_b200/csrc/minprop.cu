@@ -67,8 +67,11 @@ constexpr uint32_t kCcGrowth = 8;       // CC label window growth per advance
 // SSSP window growth per advance.  RMAT-24 (40% HBM budget), window 8:
 // fixed windows need 85 iterations and ~20 bitmap scans; growth 8 needs 19
 // iterations for the same edges expanded (10.4 -> 7.7 ms); growth 16 (18
-// iterations) measured 1.3% faster than 8 over ten sources.
-constexpr uint32_t kSsspGrowth = 16;
+// iterations) measured 1.3% faster than 8 over ten sources.  With the link
+// warps, at sources 1 / 7 / 1000 / 2: growth 8 5.61 / 7.02 / 7.40 / 6.60
+// ms, 16 5.56 / 6.92 / 7.37 / 6.45, 32 5.52 / 6.88 / 7.33 / 6.42 (15
+// iterations), 64 5.52 / 6.90 / 7.30 / 6.42.
+constexpr uint32_t kSsspGrowth = 32;
 // Direction-optimising BFS switch factors (Beamer et al., SC'12): go
 // bottom-up when the frontier's out-edges exceed the unexplored edges /
 // alpha, back to top-down when the frontier falls below nv / beta.  Alpha 4
@@ -903,51 +906,54 @@ __device__ __forceinline__ void q_append(const MinArgs &a, const uint32_t *vb,
   unsigned long long eaddr = 0;
   bool host = false;
   if (flag) {
+    // the block (shared memory) and, for a host block, the small-list
+    // cache slot depend on w alone: that load travels with the offsets'
+    const uint32_t bi = find_block(vb, a.nblk, w);
+    const unsigned long long bb = bbase[bi];
+    const bool host_blk = bb == a.host_base;
+    const uint32_t slot = host_blk && a.lc.deg_lt ? __ldg(a.lc.idx + w) : 0u;
     const uint64_t s0 = __ldg(a.off + w), e0 = __ldg(a.off + w + 1);
     deg = (uint32_t)(e0 - s0);
-    const uint32_t bi = find_block(vb, a.nblk, w);
-    eaddr = list_addr(a.lc, bbase[bi], a.host_base, w, s0, deg, ESZ, &host);
+    if (host_blk && deg > 0 && deg < a.lc.deg_lt) {
+      eaddr = a.lc.base + (unsigned long long)slot * ESZ;
+    } else {
+      host = host_blk;
+      eaddr = bb + s0 * ESZ;
+    }
     if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
   }
   const bool small = flag && deg > 0 && deg < a.small_deg;
   const bool big = flag && deg >= a.small_deg;
-  const unsigned sm = __ballot_sync(kFull, small);
-  if (sm) {
-    const int ldr = __ffs(sm) - 1;
-    unsigned long long base = 0;
-    if (lane == (unsigned)ldr) base = atomicAdd(&c->cnt_small[cs], (unsigned long long)__popc(sm));
-    base = shfl64(base, ldr);
-    const unsigned long long pos = base + __popc(sm & lanemask_lt());
-    if (small) {
-      if (pos < a.cap_s) qs[pos] = make_item(eaddr, deg, w, wval);
-      else atomicCAS(&c->err, 0u, kDevErrQueue);
-    }
-  }
-  // chunks of HBM lists fill the chunk queue from the bottom, chunks of
+  // Chunks of HBM lists fill the chunk queue from the bottom, chunks of
   // host-resident lists from the top (the expansion hands them to the
   // link warps first); the two counts together stay within cap_b, which
-  // every block checks after the phase's barrier, before any item is read
-#pragma unroll
-  for (int on_host = 0; on_host < 2; on_host++) {
-    const bool mine = big && host == (on_host != 0);
-    if (!__any_sync(kFull, mine)) continue;
-    const unsigned nch = mine ? (deg + a.chunk - 1) / a.chunk : 0u;
-    const unsigned inc = warp_incl_scan<unsigned>(nch);
-    const unsigned tot = __shfl_sync(kFull, inc, 31);
-    unsigned long long base = 0;
-    if (lane == 0)
-      base = atomicAdd(on_host ? &c->cnt_host[cs] : &c->cnt_big[cs], (unsigned long long)tot);
-    base = shfl64(base, 0);
-    if (mine) {
-      unsigned long long pos = base + inc - nch;
-      for (unsigned k = 0; k < nch; k++, pos++) {
-        const uint32_t lo = k * a.chunk;
-        if (pos < a.cap_b)
-          qb[on_host ? a.cap_b - 1 - pos : pos] =
-              make_item(eaddr + (unsigned long long)lo * ESZ, min(a.chunk, deg - lo), w, wval);
-        else
-          atomicCAS(&c->err, 0u, kDevErrQueue);
-      }
+  // every block checks after the phase's barrier, before any item is read.
+  // The three reservations (small items, HBM chunks, host chunks) go out
+  // together from lanes 0, 1 and 2.
+  const unsigned sm = __ballot_sync(kFull, small);
+  const unsigned nch = big ? (deg + a.chunk - 1) / a.chunk : 0u;
+  const unsigned inc_r = warp_incl_scan<unsigned>(host ? 0u : nch);
+  const unsigned inc_h = warp_incl_scan<unsigned>(host ? nch : 0u);
+  const unsigned tot_r = __shfl_sync(kFull, inc_r, 31), tot_h = __shfl_sync(kFull, inc_h, 31);
+  unsigned long long base = 0;
+  if (lane == 0 && sm) base = atomicAdd(&c->cnt_small[cs], (unsigned long long)__popc(sm));
+  if (lane == 1 && tot_r) base = atomicAdd(&c->cnt_big[cs], (unsigned long long)tot_r);
+  if (lane == 2 && tot_h) base = atomicAdd(&c->cnt_host[cs], (unsigned long long)tot_h);
+  const unsigned long long b_s = shfl64(base, 0), b_r = shfl64(base, 1), b_h = shfl64(base, 2);
+  if (small) {
+    const unsigned long long pos = b_s + __popc(sm & lanemask_lt());
+    if (pos < a.cap_s) qs[pos] = make_item(eaddr, deg, w, wval);
+    else atomicCAS(&c->err, 0u, kDevErrQueue);
+  }
+  if (big) {
+    unsigned long long pos = host ? b_h + inc_h - nch : b_r + inc_r - nch;
+    for (unsigned k = 0; k < nch; k++, pos++) {
+      const uint32_t lo = k * a.chunk;
+      if (pos < a.cap_b)
+        qb[host ? a.cap_b - 1 - pos : pos] =
+            make_item(eaddr + (unsigned long long)lo * ESZ, min(a.chunk, deg - lo), w, wval);
+      else
+        atomicCAS(&c->err, 0u, kDevErrQueue);
     }
   }
 }
@@ -1014,27 +1020,37 @@ __device__ __forceinline__ void q_relax_n(const MinArgs &a, const QEnv &e, const
   uint32_t r[N];
 #pragma unroll
   for (int j = 0; j < N; j++) r[j] = ok[j] ? ldcg_hint(a.val + w[j], keep) : 0u;
-#pragma unroll
-  for (int j = 0; j < N; j++)
-    r[j] = ok[j] && cand[j] < r[j] ? atomic_min_hint(a.val + w[j], cand[j], keep) : 0u;
   bool push[N];
-#pragma unroll
-  for (int j = 0; j < N; j++) {
-    const bool imp = cand[j] < r[j];  // 0 when not attempted
-    push[j] = imp && (OP == OP_BFS || cand[j] < e.thr);
-    if (OP != OP_BFS && imp && !push[j]) {
-      // parked: fire-and-forget updates (nothing waits on them)
-      atomicMin(a.wmin + (w[j] >> 5), cand[j]);
-      atomicOr(a.bm + (w[j] >> 5), 1u << (w[j] & 31u));
-    }
-  }
-  if (OP != OP_BFS) {
-    // push only if w's queued bit was clear: claim it
+  if (OP == OP_BFS) {
+    // the discoverer is the one whose atomicMin lowered the value
 #pragma unroll
     for (int j = 0; j < N; j++)
-      r[j] = push[j] ? atomicOr(e.qnext + (w[j] >> 5), 1u << (w[j] & 31u)) : 0xFFFFFFFFu;
+      r[j] = ok[j] && cand[j] < r[j] ? atomic_min_hint(a.val + w[j], cand[j], keep) : 0u;
 #pragma unroll
-    for (int j = 0; j < N; j++) push[j] = push[j] && !((r[j] >> (w[j] & 31u)) & 1u);
+    for (int j = 0; j < N; j++) push[j] = cand[j] < r[j];  // 0 when not attempted
+  } else {
+    // SSSP/CC: an edge whose candidate beats the probed value lowers it
+    // fire-and-forget, and a near one claims w's queued bit in the same
+    // round trip, before the atomicMin's outcome is known: a claim that
+    // finds the bit clear pushes w even if a concurrent relaxation lowered
+    // val[w] below the candidate first.  Then that relaxation (also near:
+    // its candidate is smaller) finds the bit set and does not push, so w
+    // is queued exactly once either way, and the expansion reads the
+    // current value.  A far candidate parks w fire-and-forget; parking
+    // after such a race only loosens the word's lower bound.
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      const bool att = ok[j] && cand[j] < r[j];
+      const bool near = att && cand[j] < e.thr;
+      r[j] = near ? atomicOr(e.qnext + (w[j] >> 5), 1u << (w[j] & 31u)) : 0xFFFFFFFFu;
+      if (att) red_min_hint(a.val + w[j], cand[j], keep);
+      if (att && !near) {
+        atomicMin(a.wmin + (w[j] >> 5), cand[j]);
+        atomicOr(a.bm + (w[j] >> 5), 1u << (w[j] & 31u));
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < N; j++) push[j] = !((r[j] >> (w[j] & 31u)) & 1u);
   }
 #pragma unroll
   for (int j = 0; j < N; j++) {

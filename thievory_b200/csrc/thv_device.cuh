@@ -79,6 +79,11 @@ __device__ __forceinline__ uint32_t ldcg_hint(const uint32_t *p, unsigned long l
   asm volatile("ld.global.cg.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
   return v;
 }
+// atomicMin whose old value nobody waits for (a reduction).
+__device__ __forceinline__ void red_min_hint(uint32_t *p, uint32_t x, unsigned long long pol) {
+  asm volatile("red.global.min.L2::cache_hint.u32 [%0], %1, %2;" : : "l"(p), "r"(x), "l"(pol)
+               : "memory");
+}
 __device__ __forceinline__ uint32_t atomic_min_hint(uint32_t *p, uint32_t x, unsigned long long pol) {
   uint32_t old;
   asm volatile("atom.global.min.L2::cache_hint.u32 %0, [%1], %2, %3;"
