@@ -46,6 +46,11 @@ enum { OP_BFS = 0, OP_CC = 1, OP_SSSP = 2 };
 
 constexpr int kMinThreads = 512;
 constexpr uint32_t kDefaultSmall = 64;  // degree < this: warp-cooperative
+// Queue mode: HBM lists of degree < this go to the small-vertex groups
+// (lists read over the link always go to chunk items).  RMAT-24 SSSP, 40%
+// HBM, sources 1 / 7 / 1000 / 2: 64 5.58 / 6.91 / 7.35 / 6.44 ms, 128 5.46
+// / 6.55 / 6.92 / 6.10, 256 5.40 / 6.50 / 6.84 / 6.04.
+constexpr uint32_t kQueueSmall = 256;
 constexpr uint32_t kDefaultChunk = 256; // edges per high-degree work item
 // Queue mode: one warp in this many (the link warps) drains the host-list
 // chunks of a phase first.  RMAT-24 SSSP, 40% HBM, mean over sources 1, 2,
@@ -922,8 +927,12 @@ __device__ __forceinline__ void q_append(const MinArgs &a, const uint32_t *vb,
     }
     if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
   }
-  const bool small = flag && deg > 0 && deg < a.small_deg;
-  const bool big = flag && deg >= a.small_deg;
+  // Lists read over the host link always go to chunk items (whole-line
+  // loads by the link warps); the small-vertex groups take only lists in
+  // HBM (resident blocks, small-list cache), whose scattered 4-byte loads
+  // would waste most of each host-link request.
+  const bool small = flag && deg > 0 && deg < a.small_deg && !host;
+  const bool big = flag && deg > 0 && !small;
   // Chunks of HBM lists fill the chunk queue from the bottom, chunks of
   // host-resident lists from the top (the expansion hands them to the
   // link warps first); the two counts together stay within cap_b, which
@@ -1678,12 +1687,25 @@ __global__ void uf_init(MinArgs a) {
 
 // ------------------------------------------------------------------ host --
 
+// Chunk items one phase can queue.  Each vertex is queued at most once per
+// phase, and a vertex of degree >= small, or (queue mode) whose list is
+// read over the host link -- a host block, degree >= the small-list cache's
+// bound -- yields ceil(deg / chunk) items: at most ne / chunk plus the
+// number of such vertices, which is at most ne / small plus the host
+// edges / the cache bound (and at most nv).
+static uint64_t chunk_capacity(const thv_graph *g, uint32_t chunk, uint32_t small) {
+  const uint64_t host_edges = g->plan.host_edge_bytes / std::max<uint32_t>(g->esz, 1);
+  const uint64_t host_lists =
+      std::min<uint64_t>(g->nv, host_edges / std::max<uint32_t>(g->plan.list_deg, 1));
+  return g->ne / chunk + g->ne / std::max<uint32_t>(small, 1) + host_lists + 64;
+}
+
 static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
                                    uint32_t small) {
   MinState *&ms = g->ms;
   // reuse the state while its chunk queue holds this configuration's items
   // (BFS/CC and SSSP default to different chunk sizes on one graph)
-  const uint64_t need_b = g->ne / chunk + g->ne / std::max<uint32_t>(small, 1) + 64;
+  const uint64_t need_b = chunk_capacity(g, chunk, small);
   if (ms && ms->valid && ms->nv == g->nv && ms->cap_b >= need_b) return THV_OK;
   if (ms) minprop_free(g);
   ms = new MinState();
@@ -1694,8 +1716,7 @@ static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
   ms->ngroups = (uint32_t)((nw + 31) / 32);
   const uint64_t nw_alloc = (uint64_t)ms->ngroups * 32;
   ms->cap_s = g->nv + 32;
-  // every pending vertex of degree >= small yields ceil(deg/chunk) items
-  ms->cap_b = g->ne / chunk + g->ne / std::max<uint32_t>(small, 1) + 64;
+  ms->cap_b = need_b;
   THV_TRY(dev_alloc((void **)&ms->d_val, g->nv * 4 + 64, "values"));
   THV_TRY(dev_alloc((void **)&ms->d_bm, nw_alloc * 4, "pending bitmap"));
   THV_TRY(dev_alloc((void **)&ms->d_wmin, nw_alloc * 4, "pending minima"));
@@ -1787,8 +1808,8 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
                        ? o->chunk_edges
                        : (queue_mode ? kQueueChunkBytes : kScanChunkBytes) / g->esz;
   chunk = std::min<uint32_t>(32768, std::max<uint32_t>(32, (chunk + 31) / 32 * 32));
-  const uint32_t small =
-      std::min<uint32_t>(32768, o && o->small_degree ? o->small_degree : kDefaultSmall);
+  const uint32_t small = std::min<uint32_t>(
+      32768, o && o->small_degree ? o->small_degree : (queue_mode ? kQueueSmall : kDefaultSmall));
   THV_TRY(ensure_plan(g));
   // work items keep edge addresses in 48 bits
   const uint64_t top = std::max<uint64_t>(g->h_edges_dev + g->h_edges_bytes,
