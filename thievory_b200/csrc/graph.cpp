@@ -733,6 +733,30 @@ thv_status build_tiles(thv_graph *g) {
     if (b.resident) p.tiles_hbm_bytes += bytes;
     else p.tiles_link_bytes += bytes;
   }
+  // Interleave host-block and HBM-block tiles in proportion to their edges.
+  // CTAs take tiles in this order from one counter, so the host link stays
+  // busy for the whole iteration while the HBM tiles are done beside it; in
+  // block order the GPU would work through host blocks with HBM idle, then
+  // HBM blocks with the link idle.  Results do not depend on the order.
+  {
+    std::vector<PrTile> host, hbm;
+    uint64_t eh = 0, er = 0;
+    for (const PrTile &t : p.tiles) {
+      if (p.blocks[t.block].resident) { hbm.push_back(t); er += t.eend - t.ebegin; }
+      else { host.push_back(t); eh += t.eend - t.ebegin; }
+    }
+    size_t i = 0, j = 0;
+    uint64_t dh = 0, dr = 0;
+    p.tiles.clear();
+    while (i < host.size() || j < hbm.size()) {
+      // take from the side that is behind its share (dh / eh vs dr / er)
+      const bool take_host =
+          j == hbm.size() || (i < host.size() && (unsigned __int128)dh * er <= (unsigned __int128)dr * eh);
+      const PrTile &t = take_host ? host[i++] : hbm[j++];
+      (take_host ? dh : dr) += t.eend - t.ebegin;
+      p.tiles.push_back(t);
+    }
+  }
   THV_TRY(dev_alloc((void **)&p.d_tiles, std::max<size_t>(1, p.tiles.size()) * sizeof(PrTile), "tiles"));
   THV_TRY(dev_alloc((void **)&p.d_split_parts, std::max<size_t>(1, p.split_parts.size()) * 4, "split table"));
   if (!p.tiles.empty())
