@@ -620,8 +620,10 @@ __global__ void __launch_bounds__(kMinThreads)
     if (leader) {
       c->cnt_small[nslot] = 0;
       c->cnt_big[nslot] = 0;
+      c->cnt_host[nslot] = 0;
       c->remaining[nslot] = 0;
       c->wc[nslot] = 0;
+      c->wc_host[nslot] = 0;
       c->minkept[nslot] = 0xFFFFFFFFu;
       c->mf[nslot] = 0;
       c->nf[nslot] = 0;
@@ -687,13 +689,13 @@ __global__ void __launch_bounds__(kMinThreads)
         else if (OP != OP_BFS && in) atomicMin(&s_km[own], vval);
         uint32_t deg = 0;
         unsigned long long eaddr = 0;
+        bool host = false;
         if (take) {
           if (OP != OP_BFS) {
             s0 = __ldg(a.off + v);
             e0 = __ldg(a.off + v + 1);
           }
           deg = (uint32_t)(e0 - s0);
-          bool host;
           const uint32_t bi = find_block(vb, a.nblk, v);
           eaddr = list_addr(a.lc, bbase[bi], a.host_base, v, s0, deg, ESZ, &host);
           if (a.blk_access) atomicAdd(a.blk_access + bi, (unsigned long long)deg * ESZ);
@@ -717,20 +719,26 @@ __global__ void __launch_bounds__(kMinThreads)
             else atomicCAS(&c->err, 0u, kDevErrQueue);
           }
         }
+        // chunks of HBM lists fill the chunk queue from the bottom, chunks
+        // of host-resident lists from the top (the link warps' pool; both
+        // counts are checked against cap_b after the barrier)
         if (__any_sync(kFull, big)) {
           const unsigned nch = big ? (deg + a.chunk - 1) / a.chunk : 0u;
-          const unsigned inc = warp_incl_scan<unsigned>(nch);
-          const unsigned tot = __shfl_sync(kFull, inc, 31);
+          const unsigned inc_r = warp_incl_scan<unsigned>(host ? 0u : nch);
+          const unsigned inc_h = warp_incl_scan<unsigned>(host ? nch : 0u);
+          const unsigned tot_r = __shfl_sync(kFull, inc_r, 31), tot_h = __shfl_sync(kFull, inc_h, 31);
           unsigned long long base = 0;
-          if (lane == 0) base = atomicAdd(&c->cnt_big[slot], (unsigned long long)tot);
-          base = shfl64(base, 0);
+          if (lane == 0 && tot_r) base = atomicAdd(&c->cnt_big[slot], (unsigned long long)tot_r);
+          if (lane == 1 && tot_h) base = atomicAdd(&c->cnt_host[slot], (unsigned long long)tot_h);
+          const unsigned long long b_r = shfl64(base, 0), b_h = shfl64(base, 1);
           if (big) {
-            unsigned long long pos = base + inc - nch;
+            unsigned long long pos = host ? b_h + inc_h - nch : b_r + inc_r - nch;
             for (unsigned kk = 0; kk < nch; kk++, pos++) {
               const uint32_t lo = kk * a.chunk;
               const uint32_t cn = min(a.chunk, deg - lo);
               if (pos < a.cap_b)
-                a.qb[pos] = make_item(eaddr + (unsigned long long)lo * ESZ, cn, v, vval);
+                a.qb[host ? a.cap_b - 1 - pos : pos] =
+                    make_item(eaddr + (unsigned long long)lo * ESZ, cn, v, vval);
               else
                 atomicCAS(&c->err, 0u, kDevErrQueue);
             }
@@ -782,7 +790,12 @@ __global__ void __launch_bounds__(kMinThreads)
 
     const unsigned long long ns = ldcg(&c->cnt_small[slot]);
     const unsigned long long nb = ldcg(&c->cnt_big[slot]);
-    if (ns + nb == 0) {
+    const unsigned long long nh = ldcg(&c->cnt_host[slot]);
+    if (nb + nh > a.cap_b) {  // the two ends of the chunk queue met
+      if (leader) atomicCAS(&c->err, 0u, kDevErrQueue);
+      break;
+    }
+    if (ns + nb + nh == 0) {
       if (OP == OP_BFS) break;
       if (ldcg(&c->remaining[slot]) == 0) break;
       const uint32_t mk = ldcg(&c->minkept[slot]);
@@ -799,23 +812,50 @@ __global__ void __launch_bounds__(kMinThreads)
     // (one task each) so that more warps share a small level's edges,
     // and groups of small vertices get smaller (down to 4 vertices)
     unsigned gsize = 32;
-    while (gsize > 4 && nb + (ns + gsize - 1) / gsize < nwarps / 2) gsize >>= 1;
+    const unsigned long long nchunks = nb + nh;
+    while (gsize > 4 && nchunks + (ns + gsize - 1) / gsize < nwarps / 2) gsize >>= 1;
     const unsigned long long ngrp = (ns + gsize - 1) / gsize;
     const unsigned parts =
-        nb && nb + ngrp < nwarps ? (unsigned)min(8ull, max(1ull, (nwarps - ngrp) / nb)) : 1u;
-    const unsigned long long nbt = nb * parts;
+        nchunks && nchunks + ngrp < nwarps
+            ? (unsigned)min(8ull, max(1ull, (nwarps - ngrp) / nchunks)) : 1u;
+    const unsigned long long nbt = nb * parts, nht = nh * parts;
     const unsigned long long ntask = nbt + ngrp;
-    for (unsigned long long t = gwarp; t < ntask;) {
-      // reserve the next task before working on this one (latency overlap)
-      unsigned long long nt = 0;
-      if (lane == 0) nt = atomicAdd(&c->wc[slot], 1ull);
-      if (t < nbt) {
-        const MinItem it = a.qb[t / parts];
-        process_chunk<OP, ESZ>(a, it, (unsigned)(t % parts), parts);
+    // Two task pools, as in queue mode: one warp in link_every drains the
+    // host-list chunks first (the link is busy from the phase's start), the
+    // others take HBM chunks and groups first; each then helps with the
+    // other pool.  First tasks are static, later ones come from the pool's
+    // counter; a warp reserves its next task before working on this one.
+    const unsigned le = a.link_every;
+    const unsigned nlink = le ? (nwarps + le - 1) / le : 0u;
+    const bool link_warp = le && gwarp % le == 0;
+#pragma unroll 1
+    for (int pass = 0; pass < 2; pass++) {
+      const bool hpool = link_warp == (pass == 0);
+      unsigned long long *ctr = hpool ? &c->wc_host[slot] : &c->wc[slot];
+      const unsigned long long n = hpool ? nht : ntask;
+      const unsigned long long first = hpool ? nlink : nwarps - nlink;
+      unsigned long long t;
+      if (pass == 0) {
+        t = link_warp ? gwarp / le : gwarp - (le ? gwarp / le + 1 : 0u);
       } else {
-        process_group<OP, ESZ>(a, (t - nbt) * gsize, ns, gsize);
+        unsigned long long f = 0;
+        if (lane == 0 && first < n) f = atomicAdd(ctr, 1ull);
+        t = first + shfl64(f, 0);
       }
-      t = nwarps + shfl64(nt, 0);
+      while (t < n) {
+        unsigned long long nt = 0;
+        if (lane == 0) nt = atomicAdd(ctr, 1ull);
+        if (hpool) {
+          const MinItem it = a.qb[a.cap_b - 1 - t / parts];
+          process_chunk<OP, ESZ>(a, it, (unsigned)(t % parts), parts);
+        } else if (t < nbt) {
+          const MinItem it = a.qb[t / parts];
+          process_chunk<OP, ESZ>(a, it, (unsigned)(t % parts), parts);
+        } else {
+          process_group<OP, ESZ>(a, (t - nbt) * gsize, ns, gsize);
+        }
+        t = first + shfl64(nt, 0);
+      }
     }
     if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
   }
