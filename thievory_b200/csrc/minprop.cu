@@ -924,17 +924,19 @@ __global__ void minprop_init(MinArgs a, uint32_t nw_alloc) {
 // each vertex once).  BFS needs neither: a vertex changes once and its
 // pusher is unique.
 
+// Expansion accounting, per warp in shared memory (registers are the
+// queue-mode kernel's limit): edges expanded and their bytes by where they
+// live.  Only lane 0 updates it.
 struct QStats {
-  unsigned long long edges = 0, hbm = 0, link = 0;
+  unsigned long long *s;  // [0] edges, [1] HBM bytes, [2] link bytes
 };
 
-// Expansion accounting: edge count and bytes by where the edges live.
 __device__ __forceinline__ void q_count(const MinArgs &a, QStats &qst, unsigned long long eaddr,
                                         unsigned cnt, unsigned esz) {
-  qst.edges += cnt;
+  qst.s[0] += cnt;
   const unsigned long long b = (unsigned long long)cnt * esz;
-  if (eaddr >= a.host_base && eaddr < a.host_end) qst.link += b;  // cache lies outside
-  else qst.hbm += b;
+  if (eaddr >= a.host_base && eaddr < a.host_end) qst.s[2] += b;  // cache lies outside
+  else qst.s[1] += b;
 }
 
 // Warp-uniform: lanes with `flag` append vertex w (value wval) to the queue
@@ -1129,11 +1131,18 @@ __device__ __forceinline__ uint32_t q_dequeue(const MinArgs &a, const QEnv &e, u
 
 template <int OP, int ESZ>
 __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const MinItem &it,
-                                        unsigned &nst, QStats &qst) {
+                                        unsigned part, unsigned parts, unsigned &nst,
+                                        QStats &qst) {
   constexpr int PER = 16 / ESZ;
   const unsigned lane = lane_id();
-  const uintptr_t start = it.ea_cnt & kAddrMask;
-  const uintptr_t end = start + (uintptr_t)(it.ea_cnt >> 48) * ESZ;
+  // part `part` of `parts` of the chunk (whole 32-edge runs): small phases
+  // split their chunks so that more warps share them
+  const uint32_t cnt = (uint32_t)(it.ea_cnt >> 48);
+  const uint32_t per = ((cnt + parts - 1) / parts + 31u) & ~31u;
+  const uint32_t lo = min(cnt, part * per), hi = min(cnt, lo + per);
+  if (lo >= hi) return;
+  const uintptr_t start = (it.ea_cnt & kAddrMask) + (uintptr_t)lo * ESZ;
+  const uintptr_t end = (it.ea_cnt & kAddrMask) + (uintptr_t)hi * ESZ;
   // two 16-byte loads per lane in flight (1 KiB per warp step): host-link
   // reads are latency-bound per warp.  The next step's loads are issued
   // before this step's relaxation, so they travel while its probes and
@@ -1158,7 +1167,7 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
     vval = __shfl_sync(kFull, vval, 0);
     if (__shfl_sync(kFull, skip, 0)) return;
   }
-  if (lane == 0) q_count(a, qst, start, (unsigned)(it.ea_cnt >> 48), ESZ);
+  if (lane == 0) q_count(a, qst, start, hi - lo, ESZ);
   if (on_link) {
 #pragma unroll
     for (int h = 0; h < 2; h++)
@@ -1191,18 +1200,28 @@ __device__ __forceinline__ void q_chunk(const MinArgs &a, const QEnv &e, const M
 template <int OP, int ESZ>
 __device__ __forceinline__ void q_group(const MinArgs &a, const QEnv &e, const MinItem *qs,
                                         unsigned long long first, unsigned long long n_small,
-                                        unsigned &nst, QStats &qst) {
+                                        unsigned gsize, unsigned &nst, QStats &qst) {
   const unsigned lane = lane_id();
   const unsigned long long idx = first + lane;
   MinItem it{0, 0, 0};
-  const bool valid = idx < n_small;
+  const bool valid = lane < gsize && idx < n_small;
   if (valid) it = qs[idx];
   bool skip = !valid;
   uint32_t vval = 0;
   if (valid) vval = q_dequeue<OP>(a, e, it.v, it.val, skip);
   const unsigned cnt = skip ? 0u : (unsigned)(it.ea_cnt >> 48);
   const unsigned long long eaddr = it.ea_cnt & kAddrMask;
-  if (cnt) q_count(a, qst, eaddr, cnt, ESZ);
+  {
+    // the group's edges and link bytes, summed over the lanes
+    const bool on_link = eaddr >= a.host_base && eaddr < a.host_end;
+    const unsigned e_sum = __reduce_add_sync(kFull, cnt);
+    const unsigned l_sum = __reduce_add_sync(kFull, on_link ? cnt : 0u);
+    if (lane == 0 && e_sum) {
+      qst.s[0] += e_sum;
+      qst.s[1] += (unsigned long long)(e_sum - l_sum) * ESZ;
+      qst.s[2] += (unsigned long long)l_sum * ESZ;
+    }
+  }
   const unsigned incl = warp_incl_scan<unsigned>(cnt);
   const unsigned excl = incl - cnt;
   const unsigned total = __shfl_sync(kFull, incl, 31);
@@ -1266,7 +1285,10 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
   uint32_t width = a.delta;
   if (OP == OP_SSSP) thr = (uint32_t)min(1ull + a.delta, 0xFFFFFFFFull);
   if (OP == OP_CC) thr = a.delta;
-  QStats qst;
+  __shared__ unsigned long long s_qst[kMinThreads / 32][3];
+  QStats qst{s_qst[threadIdx.x >> 5]};
+  if (lane < 3) qst.s[lane] = 0;
+  __syncwarp();
   // Every phase (scan or expansion) ph produces the queue in counter slot
   // ph % 3 and buffer ph & 1; an expansion consumes what phase ph - 1
   // produced.  The decision after a phase reads only that phase's slot,
@@ -1388,7 +1410,18 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
       const unsigned long long ns = ldcg(&c->cnt_small[prev]);
       const unsigned long long nb = ldcg(&c->cnt_big[prev]);
       const unsigned long long nh = ldcg(&c->cnt_host[prev]);
-      const unsigned long long ntask = nb + (ns + 31) / 32;
+      // With fewer tasks than warps (the small phases at a window's start
+      // and end), groups shrink down to 4 vertices and each chunk is split
+      // into up to 8 parts, so that more warps share the phase's edges.
+      const unsigned long long nchunks = nb + nh;
+      unsigned gsize = 32;
+      while (gsize > 4 && nchunks + (ns + gsize - 1) / gsize < nwarps / 2) gsize >>= 1;
+      const unsigned long long ngrp = (ns + gsize - 1) / gsize;
+      const unsigned parts =
+          nchunks && nchunks + ngrp < nwarps
+              ? (unsigned)min(8ull, max(1ull, (nwarps - ngrp) / nchunks)) : 1u;
+      const unsigned long long nbt = nb * parts, nht = nh * parts;
+      const unsigned long long ntask = nbt + ngrp;
       const unsigned le = a.link_every;
       const unsigned nlink = le ? (nwarps + le - 1) / le : 0u;
       const bool link_warp = le && gwarp % le == 0;
@@ -1397,7 +1430,7 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
       for (int pass = 0; pass < 2; pass++) {
         const bool hpool = link_warp == (pass == 0);
         unsigned long long *ctr = hpool ? &c->wc_host[prev] : &c->wc[prev];
-        const unsigned long long n = hpool ? nh : ntask;
+        const unsigned long long n = hpool ? nht : ntask;
         const unsigned long long first = hpool ? nlink : nwarps - nlink;
         unsigned long long t;
         if (pass == 0) {
@@ -1411,13 +1444,13 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
           unsigned long long nt = 0;
           if (lane == 0) nt = atomicAdd(ctr, 1ull);
           if (hpool) {
-            const MinItem it = qb_in[a.cap_b - 1 - t];
-            q_chunk<OP, ESZ>(a, env, it, nst, qst);
-          } else if (t < nb) {
-            const MinItem it = qb_in[t];
-            q_chunk<OP, ESZ>(a, env, it, nst, qst);
+            const MinItem it = qb_in[a.cap_b - 1 - t / parts];
+            q_chunk<OP, ESZ>(a, env, it, (unsigned)(t % parts), parts, nst, qst);
+          } else if (t < nbt) {
+            const MinItem it = qb_in[t / parts];
+            q_chunk<OP, ESZ>(a, env, it, (unsigned)(t % parts), parts, nst, qst);
           } else {
-            q_group<OP, ESZ>(a, env, qs_in, (t - nb) * 32ull, ns, nst, qst);
+            q_group<OP, ESZ>(a, env, qs_in, (t - nbt) * gsize, ns, gsize, nst, qst);
           }
           t = first + shfl64(nt, 0);
         }
@@ -1442,13 +1475,11 @@ __global__ void __launch_bounds__(kMinThreads, 2) minq_kernel(MinArgs a) {
       thr = (uint32_t)min((unsigned long long)mk + width, 0xFFFFFFFFull);
     }
   }
-  qst.edges = warp_sum(qst.edges);
-  qst.hbm = warp_sum(qst.hbm);
-  qst.link = warp_sum(qst.link);
-  if (lane == 0 && qst.edges) {
-    atomicAdd(&c->edges, qst.edges);
-    atomicAdd(&c->hbm_bytes, qst.hbm);
-    atomicAdd(&c->link_bytes, qst.link);
+  __syncwarp();
+  if (lane == 0 && qst.s[0]) {
+    atomicAdd(&c->edges, qst.s[0]);
+    atomicAdd(&c->hbm_bytes, qst.s[1]);
+    atomicAdd(&c->link_bytes, qst.s[2]);
   }
   if (leader) c->iters = iter;
 }
