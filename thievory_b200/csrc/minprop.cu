@@ -83,6 +83,9 @@ constexpr uint32_t kSsspGrowth = 32;
 // instead of the paper's 14: on RMAT-20..24 sources, 14 and 30 sometimes
 // switch a level early and scan 4-8x more in-edges (0.38 vs 0.73 ms).
 constexpr uint32_t kBfsAlpha = 4, kBfsBeta = 24;
+// Bottom-up BFS: in-edges (and their frontier words) loaded at once per
+// lane.
+constexpr int kBuBatch = 4;
 
 
 // Frontier work item of the single-source engine: the adjacency of vertex v
@@ -370,12 +373,22 @@ __device__ __noinline__ void bfs_bottom_up(const uint64_t *in_off, const uint32_
     bool found = false;
     if (v < nv && ldcg(val + v) == nv + 1u) {
       const uint64_t s = __ldg(in_off + v), e = __ldg(in_off + v + 1);
-      for (uint64_t k = s; k < e; k++) {
-        const uint32_t u = __ldg(in_adj + k);
-        scanned++;
-        if ((ldcg(front + (u >> 5)) >> (u & 31u)) & 1u) {
-          found = true;
-          break;
+      // kBuBatch in-edges and then their frontier words in flight at once
+      // (one load pair per edge in turn made a lane's scan a chain of
+      // dependent round trips); edges count up to the parent found
+      for (uint64_t k = s; k < e && !found; k += kBuBatch) {
+        uint32_t u[kBuBatch], fw[kBuBatch];
+#pragma unroll
+        for (int j = 0; j < kBuBatch; j++) u[j] = k + j < e ? __ldg(in_adj + k + j) : 0xFFFFFFFFu;
+#pragma unroll
+        for (int j = 0; j < kBuBatch; j++)
+          fw[j] = u[j] != 0xFFFFFFFFu ? ldcg(front + (u[j] >> 5)) : 0u;
+#pragma unroll
+        for (int j = 0; j < kBuBatch; j++) {
+          if (!found && u[j] != 0xFFFFFFFFu) {
+            scanned++;
+            found = (fw[j] >> (u[j] & 31u)) & 1u;
+          }
         }
       }
       if (found) {
