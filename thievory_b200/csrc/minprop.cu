@@ -86,6 +86,10 @@ constexpr uint32_t kBfsAlpha = 4, kBfsBeta = 24;
 // Bottom-up BFS: in-edges (and their frontier words) loaded at once per
 // lane.
 constexpr int kBuBatch = 4;
+// Direction-optimising BFS: a top-down level whose frontier holds at most
+// this many vertices and out-edges runs inside one CTA, with block
+// barriers, and so do the levels after it while they stay that small.
+constexpr uint32_t kLocalCap = 2048;
 
 
 // Frontier work item of the single-source engine: the adjacency of vertex v
@@ -116,6 +120,10 @@ struct MinCtrl {
   // queue mode: chunk items of host-resident lists (counted apart, stored
   // from the top of the chunk queue down) and their work counters
   unsigned long long cnt_host[3], wc_host[3];
+  // direction-optimising BFS: vertices found per level while the level is
+  // small enough to list them, and what a run of one-CTA levels hands back
+  unsigned fl_cnt[3], loc_levels;
+  unsigned long long loc_mu;
 };
 
 struct MinArgs {
@@ -151,6 +159,9 @@ struct MinArgs {
   uint32_t do_alpha, do_beta;
   // queue mode: one warp in link_every draws host-list chunks first (0: none)
   uint32_t link_every, pad3;
+  // direction-optimising BFS: lists of small frontiers (3 slots of
+  // kLocalCap vertices)
+  uint32_t *flist;
 };
 
 struct MinState {
@@ -159,6 +170,7 @@ struct MinState {
   uint32_t *d_bm = nullptr;
   uint32_t *d_wmin = nullptr;
   uint32_t *d_bm2 = nullptr;  // BFS frontier copy for bottom-up levels
+  uint32_t *d_flist = nullptr;  // BFS small-frontier lists
   MinItem *d_qs = nullptr, *d_qb = nullptr;
   MinItem *d_qs2 = nullptr, *d_qb2 = nullptr;
   uint32_t *d_qbits = nullptr;
@@ -202,6 +214,8 @@ __device__ __forceinline__ void activate(const MinArgs &a, uint32_t w,
 struct NextLevel {
   uint32_t *bits;
   unsigned long long nf, mf;
+  uint32_t *list;      // found vertices are listed here too (or null)
+  unsigned *list_cnt;  // their count; the level's out-edges bound it by kLocalCap
 };
 
 // Relax N edges at once: all value probes are issued before any atomic so a
@@ -231,6 +245,7 @@ __device__ __forceinline__ void relax_n(const MinArgs &a, const uint32_t (&w)[N]
       if (!(ldcg(bp) & m)) atomicOr(bp, m);
       nl->nf++;
       nl->mf += deg[j];
+      if (nl->list) nl->list[atomicAdd(nl->list_cnt, 1u)] = w[j];
     }
   } else {
 #pragma unroll
@@ -415,6 +430,129 @@ __device__ __noinline__ void bfs_bottom_up(const uint64_t *in_off, const uint32_
   }
 }
 
+// Top-down BFS levels inside one CTA (its threads only; the other CTAs
+// wait at the grid barrier).  The frontier of the first level is the list
+// `list_in` (n_in <= kLocalCap vertices, value lv); its bits are cleared
+// from F, each level relaxes its out-edges (at most kLocalCap) edge-parallel
+// over the block, found vertices (value lv + 1, ...) form the next list in
+// shared memory, and the run stops at a frontier that is empty, holds more
+// than kLocalCap out-edges, or would go bottom-up (out-edges x alpha above
+// the unexplored edges).  That frontier's bits are set in F and its size and
+// out-edges returned; *levels counts the levels run, *edges their
+// out-edges, and *mu comes back with the out-edges of every frontier after
+// the first and before the last taken off (as the grid's levels do).
+// Scalar arguments: a MinArgs reference would copy the kernel's parameter
+// block to local memory.
+template <int ESZ>
+__device__ __noinline__ void bfs_local_levels(const uint64_t *off, const uint32_t *vb,
+                                              const unsigned long long *bbase, uint32_t nblk,
+                                              uint32_t wshift, uint32_t *val, uint32_t *F,
+                                              const uint32_t *list_in, uint32_t n_in,
+                                              uint32_t src, uint32_t lv, uint32_t alpha,
+                                              unsigned long long *mu, unsigned *levels,
+                                              unsigned long long *edges, unsigned *nf_out,
+                                              unsigned long long *mf_out) {
+  __shared__ uint32_t s_fr[2][kLocalCap];
+  __shared__ unsigned long long s_ea[kLocalCap];
+  __shared__ uint32_t s_pre[kLocalCap + 1];
+  __shared__ uint32_t s_wsum[32];
+  __shared__ uint32_t s_n;
+  __shared__ unsigned long long s_mf;
+  const unsigned tid = threadIdx.x, nt = blockDim.x, lane = lane_id(), warp = tid >> 5;
+  for (uint32_t i = tid; i < n_in; i += nt) {
+    const uint32_t v = list_in ? list_in[i] : src;  // no list: the source alone
+    s_fr[0][i] = v;
+    atomicAnd(F + (v >> 5), ~(1u << (v & 31u)));
+  }
+  unsigned cur = 0, run = 0;
+  uint32_t n = n_in;
+  unsigned long long m = *mu, ed = 0, mf_next = 0;
+  for (;;) {
+    if (tid == 0) {
+      s_n = 0;
+      s_mf = 0;
+    }
+    __syncthreads();
+    // degrees and list addresses of this frontier; exclusive scan of the
+    // degrees, kLocalCap / blockDim.x consecutive entries per thread
+    const uint32_t per = (kLocalCap + nt - 1) / nt;
+    const uint32_t i0 = tid * per;
+    uint32_t dsum = 0;
+    for (uint32_t i = i0; i < i0 + per && i < n; i++) {
+      const uint32_t v = s_fr[cur][i];
+      const uint64_t s0 = __ldg(off + v), e0 = __ldg(off + v + 1);
+      s_pre[i] = (uint32_t)(e0 - s0);
+      s_ea[i] = bbase[find_block(vb, nblk, v)] + s0 * ESZ;
+      dsum += (uint32_t)(e0 - s0);
+    }
+    const uint32_t incl = warp_incl_scan<uint32_t>(dsum);
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t x = lane < nt / 32 ? s_wsum[lane] : 0u;
+      const uint32_t xi = warp_incl_scan<uint32_t>(x);
+      if (lane < nt / 32) s_wsum[lane] = xi - x;
+    }
+    __syncthreads();
+    uint32_t run_sum = s_wsum[warp] + incl - dsum;
+    for (uint32_t i = i0; i < i0 + per && i < n; i++) {
+      const uint32_t d = s_pre[i];
+      s_pre[i] = run_sum;
+      run_sum += d;
+    }
+    if (tid == nt - 1) s_pre[n] = run_sum;  // the last thread's end is the total
+    __syncthreads();
+    const uint32_t total = s_pre[n];
+    // edge-parallel relaxation: edge e belongs to the last vertex o with
+    // s_pre[o] <= e
+    for (uint32_t e = tid; e < total; e += nt) {
+      uint32_t lo = 0, hi = n;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_pre[mid] <= e) lo = mid;
+        else hi = mid;
+      }
+      const uintptr_t ea = (uintptr_t)s_ea[lo] + (uintptr_t)(e - s_pre[lo]) * ESZ;
+      const uint32_t raw = ld_nc_u32(ea);
+      const uint32_t w = ESZ == 4 ? edge_dst(raw, wshift) : raw;
+      if (ldcg(val + w) > lv + 1u && atomicMin(val + w, lv + 1u) > lv + 1u)
+        s_fr[cur ^ 1u][atomicAdd(&s_n, 1u)] = w;  // at most total <= kLocalCap
+    }
+    __syncthreads();
+    const uint32_t nn = s_n;
+    unsigned long long mfl = 0;
+    for (uint32_t i = tid; i < nn; i += nt) {
+      const uint32_t w = s_fr[cur ^ 1u][i];
+      mfl += __ldg(off + w + 1) - __ldg(off + w);
+    }
+    mfl = warp_sum(mfl);
+    if (lane == 0 && mfl) atomicAdd(&s_mf, mfl);
+    __syncthreads();
+    mf_next = s_mf;
+    ed += total;
+    run++;
+    const unsigned long long m_next = m > mf_next ? m - mf_next : 0ull;
+    if (nn == 0 || mf_next > kLocalCap || mf_next * alpha > m_next) {
+      // hand the frontier back to the grid as bits
+      for (uint32_t i = tid; i < nn; i += nt) {
+        const uint32_t w = s_fr[cur ^ 1u][i];
+        atomicOr(F + (w >> 5), 1u << (w & 31u));
+      }
+      *nf_out = nn;
+      break;
+    }
+    m = m_next;
+    n = nn;
+    cur ^= 1u;
+    lv++;
+    __syncthreads();
+  }
+  *mu = m;
+  *levels = run;
+  *edges = ed;
+  *mf_out = mf_next;
+}
+
 // Direction-optimising BFS on a graph whose out-edges are all resident,
 // with an in-edge transpose in HBM.  The frontier is double-buffered (F:
 // this level's, N: the next one's), and each level's direction is decided
@@ -454,6 +592,7 @@ __global__ void __launch_bounds__(kMinThreads, 2) bfs_do_kernel(MinArgs a) {
   unsigned long long mu = a.ne;      // out-edges of vertices not yet reached
   unsigned long long last_scan = 0;  // in-edges scanned by the last bottom-up level
   bool bottom_up = false;
+  bool listed = false;  // the last level listed the vertices it found
   const unsigned long long src_deg = __ldg(a.off + a.src + 1) - __ldg(a.off + a.src);
   unsigned iter = 0;
   for (;; ++iter) {
@@ -475,6 +614,7 @@ __global__ void __launch_bounds__(kMinThreads, 2) bfs_do_kernel(MinArgs a) {
       c->wc[zslot] = 0;
       c->mf[zslot] = 0;
       c->nf[zslot] = 0;
+      c->fl_cnt[zslot] = 0;
       c->bu_scan[nslot] = 0;
     }
     const unsigned long long nf = iter == 0 ? 1ull : ldcg(&c->nf[slot]);
@@ -483,12 +623,48 @@ __global__ void __launch_bounds__(kMinThreads, 2) bfs_do_kernel(MinArgs a) {
     mu = mu > mf ? mu - mf : 0;
     bottom_up = bottom_up ? nf * a.do_beta >= a.nv && 2 * mf > last_scan : mf * a.do_alpha > mu;
     const uint32_t lval = iter + 1u;  // value of this level's vertices
+    if (!bottom_up && a.flist && (iter == 0 || listed) && nf <= kLocalCap && mf <= kLocalCap) {
+      // a small top-down level (and the small ones after it) in CTA 0,
+      // while the others wait at one grid barrier instead of two per level
+      if (blockIdx.x == 0) {
+        unsigned long long lmu = mu, led = 0, lmf = 0;
+        unsigned lk = 0, lnf = 0;
+        bfs_local_levels<ESZ>(a.off, vb, bbase, a.nblk, a.wshift, a.val, F,
+                              iter == 0 ? nullptr : a.flist + slot * kLocalCap, (uint32_t)nf,
+                              a.src, lval, a.do_alpha, &lmu, &lk, &led, &lnf, &lmf);
+        if (threadIdx.x == 0) {
+          atomicAdd(&c->edges, led);
+          atomicAdd(&c->hbm_bytes, led * ESZ);  // every list is resident here
+          // the grid resumes at level iter + lk with clean counters and
+          // that level's frontier size and out-edges in its slot
+          for (int k = 0; k < 3; k++) {
+            c->cnt_small[k] = 0;
+            c->cnt_big[k] = 0;
+            c->wc[k] = 0;
+            c->mf[k] = 0;
+            c->nf[k] = 0;
+            c->bu_scan[k] = 0;
+            c->fl_cnt[k] = 0;
+          }
+          c->nf[(iter + lk) % 3] = lnf;
+          c->mf[(iter + lk) % 3] = lmf;
+          c->loc_levels = lk;
+          c->loc_mu = lmu;
+        }
+      }
+      if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
+      mu = ldcg(&c->loc_mu);
+      iter += ldcg(&c->loc_levels) - 1u;  // the loop's ++iter completes the jump
+      listed = false;
+      continue;  // F already holds the next level's frontier
+    }
     if (bottom_up) {
       bfs_bottom_up(a.in_off, a.in_adj, a.off, F, N, a.val, a.nv, lval + 1u, &c->edges,
                     &c->bu_scan[slot], &c->nf[nslot], &c->mf[nslot], gwarp, nwarps);
       if (leader) c->bu_levels++;
       if (!grid_sync(&c->bar, &c->err, a.timeout_ns)) break;
       last_scan = ldcg(&c->bu_scan[slot]);
+      listed = false;
     } else {
       if (leader) atomicAdd(&c->edges, mf);
       // ------------------------------------------------------ compaction
@@ -570,7 +746,10 @@ __global__ void __launch_bounds__(kMinThreads, 2) bfs_do_kernel(MinArgs a) {
       const unsigned parts =
           nb && nb + ngrp < nwarps ? (unsigned)min(8ull, max(1ull, (nwarps - ngrp) / nb)) : 1u;
       const unsigned long long nbt = nb * parts, ntask = nbt + ngrp;
-      NextLevel nl{N, 0, 0};
+      // a level with few out-edges also lists the vertices it finds, so
+      // that the next level can run in one CTA
+      listed = a.flist && mf <= kLocalCap;
+      NextLevel nl{N, 0, 0, listed ? a.flist + nslot * kLocalCap : nullptr, &c->fl_cnt[nslot]};
       for (unsigned long long t = gwarp; t < ntask;) {
         unsigned long long nt = 0;
         if (lane == 0) nt = atomicAdd(&c->wc[slot], 1ull);
@@ -1805,6 +1984,7 @@ static thv_status ensure_min_state(thv_graph *g, uint32_t chunk,
   THV_TRY(dev_alloc((void **)&ms->d_bm, nw_alloc * 4, "pending bitmap"));
   THV_TRY(dev_alloc((void **)&ms->d_wmin, nw_alloc * 4, "pending minima"));
   THV_TRY(dev_alloc((void **)&ms->d_bm2, nw_alloc * 4, "frontier copy"));
+  THV_TRY(dev_alloc((void **)&ms->d_flist, 3 * kLocalCap * 4, "small-frontier lists"));
   THV_TRY(dev_alloc((void **)&ms->d_qs, ms->cap_s * sizeof(MinItem), "queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qb, ms->cap_b * sizeof(MinItem), "chunk queue"));
   THV_TRY(dev_alloc((void **)&ms->d_qs2, ms->cap_s * sizeof(MinItem), "queue"));
@@ -1825,6 +2005,7 @@ void minprop_free(thv_graph *g) {
   dev_free(ms->d_bm);
   dev_free(ms->d_wmin);
   dev_free(ms->d_bm2);
+  dev_free(ms->d_flist);
   dev_free(ms->d_qs);
   dev_free(ms->d_qb);
   dev_free(ms->d_qs2);
@@ -1951,6 +2132,7 @@ thv_status run_minprop(thv_graph *g, thv_algo algo, const thv_run_opts *o,
     a.in_off = g->d_in_off;
     a.in_adj = g->d_in_adj;
     a.bm2 = ms->d_bm2;
+    a.flist = ms->d_flist;
     a.do_alpha = kBfsAlpha;
     a.do_beta = kBfsBeta;
   }
