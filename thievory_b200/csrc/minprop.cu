@@ -383,11 +383,30 @@ __device__ __noinline__ void bfs_bottom_up(const uint64_t *in_off, const uint32_
   const unsigned lane = lane_id();
   const uint32_t nwords = (nv + 31) / 32;
   unsigned long long scanned = 0, nf = 0, mf = 0;
+  // a vertex's value, in-edge range and out-edge range load together, and
+  // those of the warp's next word load before this word's scan
+  uint32_t nval = 0;
+  uint64_t ns = 0, ne = 0, nos = 0, noe = 0;
+  auto prefetch = [&](uint32_t w) {
+    const uint32_t v = w * 32u + lane;
+    if (w < nwords && v < nv) {
+      nval = ldcg(val + v);
+      ns = __ldg(in_off + v);
+      ne = __ldg(in_off + v + 1);
+      nos = __ldg(off + v);
+      noe = __ldg(off + v + 1);
+    } else {
+      nval = 0;  // not a vertex: nothing to scan
+    }
+  };
+  prefetch(gwarp);
   for (uint32_t w = gwarp; w < nwords; w += nwarps) {
     const uint32_t v = w * 32u + lane;
+    const uint32_t cval = nval;
+    const uint64_t s = ns, e = ne, os = nos, oe = noe;
+    prefetch(w + nwarps);
     bool found = false;
-    if (v < nv && ldcg(val + v) == nv + 1u) {
-      const uint64_t s = __ldg(in_off + v), e = __ldg(in_off + v + 1);
+    if (v < nv && cval == nv + 1u) {
       // kBuBatch in-edges and then their frontier words in flight at once
       // (one load pair per edge in turn made a lane's scan a chain of
       // dependent round trips); edges count up to the parent found
@@ -409,7 +428,7 @@ __device__ __noinline__ void bfs_bottom_up(const uint64_t *in_off, const uint32_
       if (found) {
         val[v] = value;
         nf++;
-        mf += __ldg(off + v + 1) - __ldg(off + v);
+        mf += oe - os;
       }
     }
     const unsigned fm = __ballot_sync(kFull, found);
